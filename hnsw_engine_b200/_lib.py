@@ -1,0 +1,111 @@
+"""ctypes binding of ``libhnsw_b200.so`` (the C ABI declared in ``include/hnsw_b200.h``).
+
+The library is built in-tree by :func:`hnsw_engine_b200.build.build`. Importing this module never
+falls back to anything else: a missing or stale library raises, so the CUDA path is the only path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libhnsw_b200.so"
+
+OK = 0
+EINVAL = -1
+ECUDA = -2
+ENOMEM = -3
+ERETRY = -4
+
+L2, IP, COSINE = 0, 1, 2
+METRIC_CODES = {"l2": L2, "ip": IP, "cosine": COSINE}
+DIST_F64 = 0
+DIST_EXACT_F32 = 1
+
+
+class Graph(ctypes.Structure):
+    _fields_ = [
+        ("vectors", ctypes.c_void_p),
+        ("codes", ctypes.c_void_p),
+        ("links0", ctypes.c_void_p),
+        ("count0", ctypes.c_void_p),
+        ("upper_offset", ctypes.c_void_p),
+        ("links_up", ctypes.c_void_p),
+        ("count_up", ctypes.c_void_p),
+        ("n", ctypes.c_int64),
+        ("rows", ctypes.c_int64),
+        ("dim", ctypes.c_int32),
+        ("links0_stride", ctypes.c_int32),
+        ("links_up_stride", ctypes.c_int32),
+        ("metric", ctypes.c_int32),
+        ("entry_point", ctypes.c_int64),
+        ("max_level", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class SearchArgs(ctypes.Structure):
+    _fields_ = [
+        ("queries", ctypes.c_void_p),
+        ("queries_f64", ctypes.c_int32),
+        ("use_codes", ctypes.c_int32),
+        ("nq", ctypes.c_int64),
+        ("k", ctypes.c_int32),
+        ("k_search", ctypes.c_int32),
+        ("ef", ctypes.c_void_p),
+        ("ef_max", ctypes.c_int32),
+        ("dist_mode", ctypes.c_int32),
+        ("allowed", ctypes.c_void_p),
+        ("allowed_fraction", ctypes.c_float),
+        ("rerank_queries", ctypes.c_void_p),
+        ("out_ids", ctypes.c_void_p),
+        ("out_dists", ctypes.c_void_p),
+        ("out_counters", ctypes.c_void_p),
+    ]
+
+
+# Every symbol include/hnsw_b200.h declares, with its ctypes signature.
+SIGNATURES: dict[str, tuple[object, list[object]]] = {
+    "hnsw_b200_open": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.POINTER(ctypes.c_void_p)]),
+    "hnsw_b200_close": (None, [ctypes.c_void_p]),
+    "hnsw_b200_search": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchArgs), ctypes.c_void_p]),
+    "hnsw_b200_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
+    "hnsw_b200_last_error": (ctypes.c_char_p, []),
+    "hnsw_b200_version": (ctypes.c_char_p, []),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+class HnswB200Error(RuntimeError):
+    """A C-ABI call failed; ``code`` is the negative status it returned."""
+
+    def __init__(self, code: int, message: str) -> None:
+        super().__init__(f"hnsw_b200 error {code}: {message}")
+        self.code = code
+
+
+def load() -> ctypes.CDLL:
+    """The loaded library with argument types set; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.is_file():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build the CUDA extension first "
+                "(python -c 'import hnsw_engine_b200.build as b; b.build()')"
+            )
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def check(code: int) -> None:
+    """Raise :class:`HnswB200Error` for a nonzero status."""
+    if code != OK:
+        msg = load().hnsw_b200_last_error()
+        raise HnswB200Error(code, msg.decode() if msg else "")

@@ -1,0 +1,1149 @@
+// Batched HNSW search on B200 (sm_100a): one warp per query, persistent grid fed by an atomic
+// work queue.
+//
+// Semantics are those of the reference's compiled search (anamankev/hnsw-engine):
+//   _search_batch            src/hnsw_engine/numba_engine.py:422-503  -> search_kernel
+//   _search_layer            numba_engine.py:98-148                    -> layer_search
+//   _search_layer0_filtered  numba_engine.py:151-198                   -> layer0_filtered
+//   _distance                numba_engine.py:57-70                     -> dist_seq_f64 / dists_exact_f32
+//   _rerank_batch            numba_engine.py:506-530                   -> rerank_epilogue
+// and the canonical rules of docs/DESIGN.md section 5 (rules 4, 5, 9): candidates pop in
+// ascending (distance, id); a neighbour is admitted iff the results hold fewer than ef entries or
+// its distance is strictly below the running worst, neighbours taken in stored link order; the
+// worst result (maximum (distance, id)) is evicted.
+//
+// Data structures (per query, one warp):
+//  * results R: a sorted (distance, id) array in shared memory with an "expanded" bit per entry.
+//    In an unfiltered layer every unexpanded result is a pending candidate, and every other pending
+//    candidate ties the worst distance (it was evicted as the maximum while the worst stayed the
+//    same), so the reference's unbounded candidate heap reduces to R plus a stack of tied ids
+//    (`ties`, popped smallest id first). Candidates farther than the worst are dropped: once the
+//    results are full the worst never grows, so the reference would stop on them.
+//  * filtered layer 0 keeps candidates explicitly (disallowed nodes are candidates but never
+//    results): a descending sorted array S in shared memory plus an unsorted global spill G whose
+//    entries all compare above every entry of S; S is refilled with the smallest entries of G.
+//  * visited: an exact open-addressing hash of node ids per warp slot in global memory (L2
+//    resident), cleared per layer, as the reference's epoch-stamped array is per layer.
+// Any capacity overflow sets a per-query status bit; the host re-runs those queries with larger
+// scratch, so results are always exact. Nothing traps and every loop is bounded.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "hnsw_b200.h"
+
+namespace hb {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int32_t EXP_BIT = int32_t(0x80000000u);
+constexpr int32_t ID_MASK = 0x7fffffff;
+constexpr int WPB = 4;  // warps per block
+
+enum : int32_t { ST_VISITED = 1, ST_TIES = 2, ST_SPILL = 4 };
+enum : int { MODE_F64 = 0, MODE_EXACT = 1 };
+
+struct SearchParams {
+    const float *vectors;
+    const uint8_t *codes;
+    const int32_t *links0;
+    const int32_t *count0;
+    const int64_t *upper_offset;
+    const int32_t *links_up;
+    const int32_t *count_up;
+    int64_t n;
+    int32_t dim, links0_stride, links_up_stride, metric;
+    int64_t entry_point;
+    int32_t max_level;
+    // batch
+    const void *queries;
+    int32_t queries_f64;
+    const int32_t *qlist;  // work item -> query row (NULL: identity)
+    int32_t n_work;
+    int32_t k, k_search;
+    const int32_t *ef;
+    int32_t ef_cap;
+    const uint32_t *allowed;
+    const float *rerank_queries;
+    int64_t *out_ids;
+    double *out_dists;
+    int64_t *out_ctr;
+    int32_t *status;
+    int32_t *n_failed;
+    int32_t *queue;
+    // scratch (per warp slot)
+    int32_t *vis;
+    int64_t vis_stride;
+    int32_t vis_log2, vis_up_log2;
+    int32_t *ties;
+    int32_t tie_cap;
+    double *spill_d;
+    int32_t *spill_i;
+    int32_t spill_cap;
+    int32_t s_cap;
+};
+
+__host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Shared memory of one warp: results, query (f64 and f32), filtered candidates, rerank top-k.
+__host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filtered, int s_cap,
+                                                  int k_rerank) {
+    size_t b = al16(size_t(ef_cap + 1) * 8) + al16(size_t(ef_cap + 1) * 4) + al16(size_t(dim) * 8) +
+               al16(size_t(dim) * 4);
+    if (filtered) b += al16(size_t(s_cap + 1) * 8) + al16(size_t(s_cap + 1) * 4);
+    if (k_rerank > 0) b += al16(size_t(k_rerank + 1) * 8) + al16(size_t(k_rerank + 1) * 4);
+    return b;
+}
+
+struct Ctx {
+    int lane;
+    double *Rd;
+    int32_t *Ri;
+    double *qd;
+    float *qf;
+    double *Sd;
+    int32_t *Si;
+    double *Ad;
+    int32_t *Ai;
+    int32_t *vis;
+    int32_t *ties;
+    double *spd;
+    int32_t *spi;
+    long long ndist, nhops;  // uniform across the warp
+    int32_t status;          // uniform across the warp
+};
+
+__device__ __forceinline__ bool pair_lt(double da, int32_t ia, double db, int32_t ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+// ---------------------------------------------------------------------------------------- sorted
+// Entries of the ascending array [0, m) strictly below (d, id).
+__device__ __forceinline__ int count_below(const double *Ad, const int32_t *Ai, int m, double d,
+                                           int32_t id, int lane) {
+    int c = 0;
+    for (int i = lane; i < m; i += 32) c += pair_lt(Ad[i], Ai[i] & ID_MASK, d, id);
+    return __reduce_add_sync(FULL, c);
+}
+
+// Entries of the descending array [0, m) strictly above (d, id).
+__device__ __forceinline__ int count_above(const double *Ad, const int32_t *Ai, int m, double d,
+                                           int32_t id, int lane) {
+    int c = 0;
+    for (int i = lane; i < m; i += 32) c += pair_lt(d, id, Ad[i], Ai[i]);
+    return __reduce_add_sync(FULL, c);
+}
+
+// Move [pos, m) to [pos + 1, m + 1), highest chunk first.
+__device__ __forceinline__ void shift_up(double *Ad, int32_t *Ai, int pos, int m, int lane) {
+    for (int top = m - 1; top >= pos; top -= 32) {
+        int i = top - lane;
+        bool act = i >= pos;
+        double d = 0.0;
+        int32_t id = 0;
+        if (act) {
+            d = Ad[i];
+            id = Ai[i];
+        }
+        __syncwarp();
+        if (act) {
+            Ad[i + 1] = d;
+            Ai[i + 1] = id;
+        }
+        __syncwarp();
+    }
+}
+
+// Move [pos + 1, m) to [pos, m - 1), lowest chunk first.
+__device__ __forceinline__ void shift_down(double *Ad, int32_t *Ai, int pos, int m, int lane) {
+    for (int base = pos; base < m - 1; base += 32) {
+        int i = base + lane;
+        bool act = i < m - 1;
+        double d = 0.0;
+        int32_t id = 0;
+        if (act) {
+            d = Ad[i + 1];
+            id = Ai[i + 1];
+        }
+        __syncwarp();
+        if (act) {
+            Ad[i] = d;
+            Ai[i] = id;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------- visited
+__device__ __forceinline__ void vis_clear(int32_t *tab, int log2, int lane) {
+    int4 *t4 = reinterpret_cast<int4 *>(tab);
+    const int n4 = (1 << log2) >> 2;
+    for (int i = lane; i < n4; i += 32) t4[i] = make_int4(0, 0, 0, 0);
+    __syncwarp();
+}
+
+// 1: inserted (was unvisited); 0: already present; -1: table full.
+__device__ __forceinline__ int vis_insert(int32_t *tab, int log2, int32_t id) {
+    const uint32_t mask = (1u << log2) - 1u;
+    uint32_t h = (uint32_t(id) * 2654435761u) >> (32 - log2);
+    const int32_t key = id + 1;
+    for (uint32_t p = 0; p <= mask; p++) {
+        int32_t old = atomicCAS(tab + h, 0, key);
+        if (old == 0) return 1;
+        if (old == key) return 0;
+        h = (h + 1u) & mask;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ bool is_allowed(const uint32_t *bits, int32_t e) {
+    return (__ldg(bits + (e >> 5)) >> (e & 31)) & 1u;
+}
+
+// -------------------------------------------------------------------------------------- distances
+// Float64, strictly sequential over the dimensions with separate multiply and add: the exact
+// arithmetic of numba_engine._distance (:57-70) for float32 or uint8 rows and a float64 query.
+template <bool U8>
+__device__ __forceinline__ double dist_seq_f64(const SearchParams &P, int64_t e, const double *q) {
+    const int dim = P.dim;
+    double acc = 0.0;
+    if (!U8) {
+        const float *x = P.vectors + e * dim;
+        if ((dim & 3) == 0) {
+            const float4 *x4 = reinterpret_cast<const float4 *>(x);
+            if (P.metric == HNSW_B200_L2) {
+                for (int i = 0; i < dim; i += 4) {
+                    float4 v = __ldg(x4 + (i >> 2));
+                    double t;
+                    t = __dsub_rn((double)v.x, q[i]);
+                    acc = __dadd_rn(acc, __dmul_rn(t, t));
+                    t = __dsub_rn((double)v.y, q[i + 1]);
+                    acc = __dadd_rn(acc, __dmul_rn(t, t));
+                    t = __dsub_rn((double)v.z, q[i + 2]);
+                    acc = __dadd_rn(acc, __dmul_rn(t, t));
+                    t = __dsub_rn((double)v.w, q[i + 3]);
+                    acc = __dadd_rn(acc, __dmul_rn(t, t));
+                }
+                return acc;
+            }
+            for (int i = 0; i < dim; i += 4) {
+                float4 v = __ldg(x4 + (i >> 2));
+                acc = __dadd_rn(acc, __dmul_rn((double)v.x, q[i]));
+                acc = __dadd_rn(acc, __dmul_rn((double)v.y, q[i + 1]));
+                acc = __dadd_rn(acc, __dmul_rn((double)v.z, q[i + 2]));
+                acc = __dadd_rn(acc, __dmul_rn((double)v.w, q[i + 3]));
+            }
+        } else {
+            if (P.metric == HNSW_B200_L2) {
+                for (int i = 0; i < dim; i++) {
+                    double t = __dsub_rn((double)__ldg(x + i), q[i]);
+                    acc = __dadd_rn(acc, __dmul_rn(t, t));
+                }
+                return acc;
+            }
+            for (int i = 0; i < dim; i++) acc = __dadd_rn(acc, __dmul_rn((double)__ldg(x + i), q[i]));
+        }
+    } else {
+        const uint8_t *x = P.codes + e * dim;
+        if (P.metric == HNSW_B200_L2) {
+            for (int i = 0; i < dim; i++) {
+                double t = __dsub_rn((double)__ldg(x + i), q[i]);
+                acc = __dadd_rn(acc, __dmul_rn(t, t));
+            }
+            return acc;
+        }
+        for (int i = 0; i < dim; i++) acc = __dadd_rn(acc, __dmul_rn((double)__ldg(x + i), q[i]));
+    }
+    return P.metric == HNSW_B200_IP ? -acc : __dsub_rn(1.0, acc);
+}
+
+__device__ __forceinline__ float4 load_row4(const SearchParams &P, int64_t e, int c, bool u8) {
+    if (!u8) return __ldg(reinterpret_cast<const float4 *>(P.vectors + e * P.dim + c));
+    uchar4 b = __ldg(reinterpret_cast<const uchar4 *>(P.codes + e * P.dim + c));
+    return make_float4(b.x, b.y, b.z, b.w);
+}
+
+__device__ __forceinline__ float row_elem(const SearchParams &P, int64_t e, int c, bool u8) {
+    return u8 ? float(__ldg(P.codes + e * P.dim + c)) : __ldg(P.vectors + e * P.dim + c);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Float32 warp-cooperative distances for integer-valued data whose partial sums stay below 2^24:
+// every product and sum is then exact, in any order, and equals the reference's float64 value.
+// Lane j (bit j of umask) receives the distance of the neighbour it holds in `e`.
+template <bool U8>
+__device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e, uint32_t umask,
+                                                const float *qf, int lane, double &dj) {
+    const int dim = P.dim;
+    const bool l2 = P.metric == HNSW_B200_L2;
+    const bool vec = (dim & 3) == 0;
+    while (umask) {
+        int jj[4];
+        int64_t ee[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            if (umask) {
+                jj[t] = __ffs(umask) - 1;
+                umask &= umask - 1;
+            } else {
+                jj[t] = -1;
+            }
+            ee[t] = __shfl_sync(FULL, e, jj[t] < 0 ? 0 : jj[t]);
+        }
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        if (vec) {
+            for (int c = lane * 4; c < dim; c += 128) {
+                float4 qv = *reinterpret_cast<const float4 *>(qf + c);
+                float4 xv[4];
+#pragma unroll
+                for (int t = 0; t < 4; t++)
+                    if (jj[t] >= 0) xv[t] = load_row4(P, ee[t], c, U8);
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    if (jj[t] < 0) continue;
+                    if (l2) {
+                        float a = xv[t].x - qv.x, b = xv[t].y - qv.y, cc = xv[t].z - qv.z,
+                              d = xv[t].w - qv.w;
+                        acc[t] = fmaf(a, a, acc[t]);
+                        acc[t] = fmaf(b, b, acc[t]);
+                        acc[t] = fmaf(cc, cc, acc[t]);
+                        acc[t] = fmaf(d, d, acc[t]);
+                    } else {
+                        acc[t] = fmaf(xv[t].x, qv.x, acc[t]);
+                        acc[t] = fmaf(xv[t].y, qv.y, acc[t]);
+                        acc[t] = fmaf(xv[t].z, qv.z, acc[t]);
+                        acc[t] = fmaf(xv[t].w, qv.w, acc[t]);
+                    }
+                }
+            }
+        } else {
+            for (int c = lane; c < dim; c += 32) {
+                float qv = qf[c];
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    if (jj[t] < 0) continue;
+                    float x = row_elem(P, ee[t], c, U8);
+                    if (l2) {
+                        float a = x - qv;
+                        acc[t] = fmaf(a, a, acc[t]);
+                    } else {
+                        acc[t] = fmaf(x, qv, acc[t]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            if (jj[t] < 0) continue;  // uniform
+            float s = warp_sum(acc[t]);
+            double d = l2 ? double(s) : (P.metric == HNSW_B200_IP ? -double(s) : 1.0 - double(s));
+            if (lane == jj[t]) dj = d;
+        }
+    }
+}
+
+// Distance of one node held uniformly by the warp.
+template <int MODE, bool U8>
+__device__ __forceinline__ double dist_one(const SearchParams &P, Ctx &C, int32_t e) {
+    double d = 0.0;
+    if (MODE == MODE_EXACT) {
+        dists_exact_f32<U8>(P, e, 1u, C.qf, C.lane, d);
+    } else if (C.lane == 0) {
+        d = dist_seq_f64<U8>(P, e, C.qd);
+    }
+    return __shfl_sync(FULL, d, 0);
+}
+
+// Mark one chunk of up to 32 neighbours visited (first occurrence wins) and score the new ones.
+// Returns the mask of lanes holding a newly visited neighbour; its distance is in dj.
+template <int MODE, bool U8>
+__device__ __forceinline__ uint32_t visit_chunk(const SearchParams &P, Ctx &C, int32_t e, int log2,
+                                                int &vis_count, double &dj) {
+    const bool has = e >= 0;
+    const uint32_t hmask = __ballot_sync(FULL, has);
+    int ins = 0;
+    if (has) {
+        uint32_t same = __match_any_sync(hmask, e);
+        if (__ffs(same) - 1 == C.lane) ins = vis_insert(C.vis, log2, e);
+    }
+    const uint32_t umask = __ballot_sync(FULL, ins == 1);
+    if (__any_sync(FULL, ins < 0)) C.status |= ST_VISITED;
+    vis_count += __popc(umask);
+    dj = 0.0;
+    if (MODE == MODE_EXACT) {
+        dists_exact_f32<U8>(P, e, umask, C.qf, C.lane, dj);
+    } else if (ins == 1) {
+        dj = dist_seq_f64<U8>(P, e, C.qd);
+    }
+    return umask;
+}
+
+__device__ __forceinline__ const int32_t *node_links(const SearchParams &P, int32_t c, int layer,
+                                                     int &cnt) {
+    if (layer == 0) {
+        cnt = __ldg(P.count0 + c);
+        return P.links0 + int64_t(c) * P.links0_stride;
+    }
+    int64_t row = __ldg(P.upper_offset + c) + layer - 1;
+    cnt = __ldg(P.count_up + row);
+    return P.links_up + row * P.links_up_stride;
+}
+
+// ------------------------------------------------------------------------- unfiltered layer search
+// Algorithm 2 with exact reference semantics. On entry R[0] holds the single entry node
+// (unexpanded) and r == 1; on exit R[0..r) is the sorted result list.
+template <int MODE, bool U8>
+__device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, int log2, int &r) {
+    const int lane = C.lane;
+    vis_clear(C.vis, log2, lane);
+    if (lane == 0) vis_insert(C.vis, log2, C.Ri[0] & ID_MASK);
+    __syncwarp();
+    int vis_count = 1;
+    const int vis_lim = ((1 << log2) >> 2) * 3;
+    double W = C.Rd[r - 1];
+    int scan = 0;  // every result before `scan` is expanded
+    int tn = 0;    // tie stack depth
+    for (;;) {
+        int32_t c = -1;
+        while (scan < r) {
+            const int i = scan + lane;
+            const bool un = i < r && !(C.Ri[i] & EXP_BIT);
+            const uint32_t b = __ballot_sync(FULL, un);
+            if (b) {
+                const int p = scan + __ffs(b) - 1;
+                c = C.Ri[p];
+                scan = p + 1;
+                __syncwarp();
+                if (lane == 0) C.Ri[p] = c | EXP_BIT;
+                __syncwarp();
+                break;
+            }
+            scan += 32;
+        }
+        if (c < 0) {
+            if (tn == 0) break;
+            tn--;
+            c = C.ties[tn];  // ties W: expanded after every result (they compare greater)
+        }
+        C.nhops++;
+        int cnt;
+        const int32_t *nb = node_links(P, c, layer, cnt);
+        for (int base = 0; base < cnt; base += 32) {
+            const int32_t e = base + lane < cnt ? __ldg(nb + base + lane) : -1;
+            double dj;
+            const uint32_t um = visit_chunk<MODE, U8>(P, C, e, log2, vis_count, dj);
+            C.ndist += __popc(um);
+            uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
+            while (am) {
+                const int j = __ffs(am) - 1;
+                am &= am - 1;
+                const double d = __shfl_sync(FULL, dj, j);
+                const int32_t id = __shfl_sync(FULL, e, j);
+                if (!(r < ef || d < W)) continue;  // uniform
+                const int pos = count_below(C.Rd, C.Ri, r, d, id, lane);
+                shift_up(C.Rd, C.Ri, pos, r, lane);
+                if (lane == 0) {
+                    C.Rd[pos] = d;
+                    C.Ri[pos] = id;
+                }
+                __syncwarp();
+                r++;
+                if (pos < scan) scan = pos;
+                if (r > ef) {  // evict the maximum (d, id)
+                    r = ef;
+                    const double ed = C.Rd[ef];
+                    const int32_t ei = C.Ri[ef];
+                    if (ed == C.Rd[ef - 1]) {
+                        if (!(ei & EXP_BIT)) {  // still a candidate, tied with the worst
+                            if (tn < P.tie_cap) {
+                                if (lane == 0) C.ties[tn] = ei;
+                                tn++;
+                            } else {
+                                C.status |= ST_TIES;
+                            }
+                        }
+                    } else {
+                        tn = 0;  // the worst dropped: every tied candidate is now too far
+                    }
+                }
+                W = C.Rd[r - 1];
+                if (r == ef) am &= __ballot_sync(FULL, dj < W);
+            }
+        }
+        if (vis_count > vis_lim) C.status |= ST_VISITED;
+        if (C.status) break;
+        __syncwarp();
+    }
+}
+
+// -------------------------------------------------------------------- filtered candidate storage
+struct Cands {
+    int s;        // entries in S (descending: S[s-1] is the minimum)
+    int g;        // entries in the global spill G
+    double gd;    // minimum (d, id) of G when g > 0
+    int32_t gi;
+};
+
+__device__ __forceinline__ void spill_push(const SearchParams &P, Ctx &C, Cands &K, double d,
+                                           int32_t id) {
+    if (K.g < P.spill_cap) {
+        if (C.lane == 0) {
+            C.spd[K.g] = d;
+            C.spi[K.g] = id;
+        }
+        K.g++;
+    } else {
+        C.status |= ST_SPILL;
+    }
+}
+
+__device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &K, double d,
+                                          int32_t id) {
+    if (K.g > 0 && !pair_lt(d, id, K.gd, K.gi)) {  // not below the spill minimum
+        spill_push(P, C, K, d, id);
+        return;
+    }
+    const int pos = count_above(C.Sd, C.Si, K.s, d, id, C.lane);
+    shift_up(C.Sd, C.Si, pos, K.s, C.lane);
+    if (C.lane == 0) {
+        C.Sd[pos] = d;
+        C.Si[pos] = id;
+    }
+    __syncwarp();
+    K.s++;
+    if (K.s > P.s_cap) {  // move the maximum to the spill; it becomes the spill minimum
+        const double md = C.Sd[0];
+        const int32_t mi = C.Si[0];
+        shift_down(C.Sd, C.Si, 0, K.s, C.lane);
+        K.s--;
+        spill_push(P, C, K, md, mi);
+        K.gd = md;
+        K.gi = mi;
+    }
+}
+
+// Refill the empty S with the smallest spill entries (at most s_cap / 2), dropping entries that
+// can no longer be expanded (distance above the worst of full results).
+__device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune, double Wp) {
+    const int lane = C.lane;
+    const int B = max(1, P.s_cap / 2);
+    int s = 0;
+    for (int base = 0; base < K.g; base += 32) {
+        const int i = base + lane;
+        double d = 0.0;
+        int32_t id = 0;
+        bool v = i < K.g;
+        if (v) {
+            d = C.spd[i];
+            id = C.spi[i];
+            if (prune && d > Wp) v = false;
+        }
+        uint32_t cm = __ballot_sync(FULL, v && (s < B || pair_lt(d, id, C.Sd[0], C.Si[0])));
+        while (cm) {
+            const int j = __ffs(cm) - 1;
+            cm &= cm - 1;
+            const double xd = __shfl_sync(FULL, d, j);
+            const int32_t xi = __shfl_sync(FULL, id, j);
+            if (!(s < B || pair_lt(xd, xi, C.Sd[0], C.Si[0]))) continue;
+            const int pos = count_above(C.Sd, C.Si, s, xd, xi, lane);
+            shift_up(C.Sd, C.Si, pos, s, lane);
+            if (lane == 0) {
+                C.Sd[pos] = xd;
+                C.Si[pos] = xi;
+            }
+            __syncwarp();
+            s++;
+            if (s > B) {
+                shift_down(C.Sd, C.Si, 0, s, lane);
+                s--;
+            }
+            if (s == B) cm &= __ballot_sync(FULL, pair_lt(d, id, C.Sd[0], C.Si[0]));
+        }
+    }
+    // Compact the spill: keep entries not selected (above S's maximum) and not pruned.
+    const double td = s > 0 ? C.Sd[0] : -INFINITY;
+    const int32_t ti = s > 0 ? C.Si[0] : -1;
+    int w = 0;
+    double md = INFINITY;
+    int32_t mi = 0x7fffffff;
+    for (int base = 0; base < K.g; base += 32) {
+        const int i = base + lane;
+        double d = 0.0;
+        int32_t id = 0;
+        bool keep = false;
+        if (i < K.g) {
+            d = C.spd[i];
+            id = C.spi[i];
+            keep = !(prune && d > Wp) && pair_lt(td, ti, d, id);
+        }
+        const uint32_t km = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep) {
+            const int o = w + __popc(km & ((1u << lane) - 1u));
+            C.spd[o] = d;
+            C.spi[o] = id;
+            if (pair_lt(d, id, md, mi)) {
+                md = d;
+                mi = id;
+            }
+        }
+        w += __popc(km);
+        __syncwarp();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double od = __shfl_xor_sync(FULL, md, o);
+        const int32_t oi = __shfl_xor_sync(FULL, mi, o);
+        if (pair_lt(od, oi, md, mi)) {
+            md = od;
+            mi = oi;
+        }
+    }
+    K.s = s;
+    K.g = w;
+    K.gd = md;
+    K.gi = mi;
+}
+
+// ----------------------------------------------------------------------- filtered layer-0 search
+// numba_engine._search_layer0_filtered (:151-198): results hold allowed nodes only, the worst of
+// an empty result list is +inf, and the search stops only when the results are full and the
+// closest candidate is strictly farther than the worst.
+template <int MODE, bool U8>
+__device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2, double d0,
+                                int32_t e0, int &r) {
+    const int lane = C.lane;
+    vis_clear(C.vis, log2, lane);
+    if (lane == 0) {
+        vis_insert(C.vis, log2, e0);
+        C.Sd[0] = d0;
+        C.Si[0] = e0;
+        if (is_allowed(P.allowed, e0)) {
+            C.Rd[0] = d0;
+            C.Ri[0] = e0;
+        }
+    }
+    __syncwarp();
+    r = is_allowed(P.allowed, e0) ? 1 : 0;
+    Cands K{1, 0, INFINITY, 0x7fffffff};
+    int vis_count = 1;
+    const int vis_lim = ((1 << log2) >> 2) * 3;
+    double W = r > 0 ? C.Rd[r - 1] : INFINITY;
+    for (;;) {
+        if (K.s == 0) {
+            if (K.g == 0) break;
+            cand_refill(P, C, K, r == ef, W);
+            if (K.s == 0) break;
+        }
+        const double dc = C.Sd[K.s - 1];
+        const int32_t c = C.Si[K.s - 1];
+        K.s--;
+        if (r == ef && dc > W) break;
+        C.nhops++;
+        const int cnt = __ldg(P.count0 + c);
+        const int32_t *nb = P.links0 + int64_t(c) * P.links0_stride;
+        for (int base = 0; base < cnt; base += 32) {
+            const int32_t e = base + lane < cnt ? __ldg(nb + base + lane) : -1;
+            double dj;
+            const uint32_t um = visit_chunk<MODE, U8>(P, C, e, log2, vis_count, dj);
+            C.ndist += __popc(um);
+            uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
+            while (am) {
+                const int j = __ffs(am) - 1;
+                am &= am - 1;
+                const double d = __shfl_sync(FULL, dj, j);
+                const int32_t id = __shfl_sync(FULL, e, j);
+                if (!(r < ef || d < W)) continue;
+                cand_push(P, C, K, d, id);
+                if (is_allowed(P.allowed, id)) {
+                    const int pos = count_below(C.Rd, C.Ri, r, d, id, lane);
+                    shift_up(C.Rd, C.Ri, pos, r, lane);
+                    if (lane == 0) {
+                        C.Rd[pos] = d;
+                        C.Ri[pos] = id;
+                    }
+                    __syncwarp();
+                    r++;
+                    if (r > ef) r = ef;
+                    W = C.Rd[r - 1];
+                }
+                if (r == ef) am &= __ballot_sync(FULL, dj < W);
+            }
+        }
+        if (vis_count > vis_lim) C.status |= ST_VISITED;
+        if (C.status) break;
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------------------ rerank epilogue
+// numba_engine._rerank_batch (:506-530): exact float64 distances from the float32 query to the
+// first m beam entries, best k by (distance, id).
+__device__ int rerank_epilogue(const SearchParams &P, Ctx &C, int m) {
+    const int lane = C.lane;
+    const int k = P.k;
+    int a = 0;
+    for (int base = 0; base < m; base += 32) {
+        const int i = base + lane;
+        const bool has = i < m;
+        const int32_t id = has ? (C.Ri[i] & ID_MASK) : -1;
+        const double d = has ? dist_seq_f64<false>(P, id, C.qd) : INFINITY;
+        uint32_t am = __ballot_sync(FULL, has);
+        while (am) {
+            const int j = __ffs(am) - 1;
+            am &= am - 1;
+            const double xd = __shfl_sync(FULL, d, j);
+            const int32_t xi = __shfl_sync(FULL, id, j);
+            if (a == k && !pair_lt(xd, xi, C.Ad[k - 1], C.Ai[k - 1])) continue;
+            const int pos = count_below(C.Ad, C.Ai, a, xd, xi, lane);
+            shift_up(C.Ad, C.Ai, pos, a, lane);
+            if (lane == 0) {
+                C.Ad[pos] = xd;
+                C.Ai[pos] = xi;
+            }
+            __syncwarp();
+            a = min(a + 1, k);
+        }
+    }
+    return a;
+}
+
+// --------------------------------------------------------------------------------------- kernel
+template <int MODE, bool U8, bool FILT>
+__global__ void __launch_bounds__(WPB * 32) search_kernel(const SearchParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const bool rerank = P.rerank_queries != nullptr;
+    const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0);
+    unsigned char *p = smem + size_t(warp) * wb;
+    Ctx C;
+    C.lane = lane;
+    C.Rd = reinterpret_cast<double *>(p);
+    p += al16(size_t(P.ef_cap + 1) * 8);
+    C.Ri = reinterpret_cast<int32_t *>(p);
+    p += al16(size_t(P.ef_cap + 1) * 4);
+    C.qd = reinterpret_cast<double *>(p);
+    p += al16(size_t(P.dim) * 8);
+    C.qf = reinterpret_cast<float *>(p);
+    p += al16(size_t(P.dim) * 4);
+    C.Sd = nullptr;
+    C.Si = nullptr;
+    if (FILT) {
+        C.Sd = reinterpret_cast<double *>(p);
+        p += al16(size_t(P.s_cap + 1) * 8);
+        C.Si = reinterpret_cast<int32_t *>(p);
+        p += al16(size_t(P.s_cap + 1) * 4);
+    }
+    C.Ad = reinterpret_cast<double *>(p);
+    p += rerank ? al16(size_t(P.k + 1) * 8) : 0;
+    C.Ai = reinterpret_cast<int32_t *>(p);
+    const int64_t slot = int64_t(blockIdx.x) * WPB + warp;
+    C.vis = P.vis + slot * P.vis_stride;
+    C.ties = P.ties + slot * P.tie_cap;
+    C.spd = FILT ? P.spill_d + slot * P.spill_cap : nullptr;
+    C.spi = FILT ? P.spill_i + slot * P.spill_cap : nullptr;
+
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = atomicAdd(P.queue, 1);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= P.n_work) break;
+        const int q = P.qlist ? P.qlist[w] : w;
+        const int dim = P.dim;
+        if (P.queries_f64) {
+            const double *src = static_cast<const double *>(P.queries) + int64_t(q) * dim;
+            for (int i = lane; i < dim; i += 32) {
+                C.qd[i] = src[i];
+                C.qf[i] = float(src[i]);
+            }
+        } else {
+            const float *src = static_cast<const float *>(P.queries) + int64_t(q) * dim;
+            for (int i = lane; i < dim; i += 32) {
+                C.qd[i] = double(src[i]);
+                C.qf[i] = src[i];
+            }
+        }
+        __syncwarp();
+        C.ndist = 0;
+        C.nhops = 0;
+        C.status = 0;
+        // Entry point, then greedy descent (ef = 1) through the upper layers.
+        int32_t e0 = int32_t(P.entry_point);
+        double d0 = dist_one<MODE, U8>(P, C, e0);
+        C.ndist++;
+        int r = 1;
+        for (int layer = P.max_level; layer > 0 && !C.status; layer--) {
+            if (lane == 0) {
+                C.Rd[0] = d0;
+                C.Ri[0] = e0;
+            }
+            __syncwarp();
+            r = 1;
+            layer_search<MODE, U8>(P, C, layer, 1, P.vis_up_log2, r);
+            d0 = C.Rd[0];
+            e0 = C.Ri[0] & ID_MASK;
+            __syncwarp();
+        }
+        const int ef0 = max(__ldg(P.ef + q), P.k_search);
+        if (!C.status) {
+            if (FILT) {
+                layer0_filtered<MODE, U8>(P, C, ef0, P.vis_log2, d0, e0, r);
+            } else {
+                if (lane == 0) {
+                    C.Rd[0] = d0;
+                    C.Ri[0] = e0;
+                }
+                __syncwarp();
+                r = 1;
+                layer_search<MODE, U8>(P, C, 0, ef0, P.vis_log2, r);
+            }
+        }
+        if (C.status) {
+            if (lane == 0) {
+                P.status[q] = C.status;
+                atomicAdd(P.n_failed, 1);
+            }
+            __syncwarp();
+            continue;
+        }
+        const int k = P.k;
+        int64_t *oi = P.out_ids + int64_t(q) * k;
+        double *od = P.out_dists + int64_t(q) * k;
+        if (rerank) {
+            const float *rq = P.rerank_queries + int64_t(q) * dim;
+            for (int i = lane; i < dim; i += 32) C.qd[i] = double(rq[i]);
+            __syncwarp();
+            const int a = rerank_epilogue(P, C, min(r, P.k_search));
+            for (int i = lane; i < k; i += 32) {
+                oi[i] = i < a ? int64_t(C.Ai[i]) : -1;
+                od[i] = i < a ? C.Ad[i] : INFINITY;
+            }
+        } else {
+            for (int i = lane; i < k; i += 32) {
+                oi[i] = i < r ? int64_t(C.Ri[i] & ID_MASK) : -1;
+                od[i] = i < r ? C.Rd[i] : INFINITY;
+            }
+        }
+        if (lane == 0) {
+            P.status[q] = 0;
+            if (P.out_ctr) {
+                P.out_ctr[2 * int64_t(q)] = C.ndist;
+                P.out_ctr[2 * int64_t(q) + 1] = C.nhops;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Collect the work items whose status is nonzero into qlist_out (order: by query row).
+__global__ void collect_failed(const int32_t *status, const int32_t *qlist, int32_t n_work,
+                               int32_t *out, int32_t *n_out) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < n_work; w += gridDim.x * blockDim.x) {
+        const int q = qlist ? qlist[w] : w;
+        if (status[q] != 0) out[atomicAdd(n_out, 1)] = q;
+    }
+}
+
+// ======================================================================================== host
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t _e = (expr);                                                           \
+        if (_e != cudaSuccess)                                                             \
+            return fail(HNSW_B200_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+struct Buffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want) {
+        if (want <= bytes) return 0;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        size_t b = std::max(want, size_t(256));
+        if (cudaMalloc(&ptr, b) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HNSW_B200_ENOMEM, "cudaMalloc of " + std::to_string(b) + " bytes failed");
+        }
+        bytes = b;
+        return 0;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+struct Handle {
+    hnsw_b200_graph_t g;
+    int device = 0;
+    int sms = 148;
+    Buffer counters;  // queue, n_failed, n_list
+    Buffer status;
+    Buffer qlist[2];  // retry work lists (ping-pong)
+    Buffer vis, ties, spill_d, spill_i;
+    int32_t *host_pinned = nullptr;  // 4 ints
+    long long launches = 0;
+    std::mutex mu;
+};
+
+template <int MODE, bool U8, bool FILT>
+int launch_one(Handle &h, const SearchParams &P, size_t smem_block, int blocks, cudaStream_t s) {
+    auto kern = search_kernel<MODE, U8, FILT>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem_block)));
+    kern<<<blocks, WPB * 32, smem_block, s>>>(P);
+    CUDA_TRY(cudaGetLastError());
+    h.launches++;
+    return 0;
+}
+
+template <int MODE, bool U8>
+int launch_mode(Handle &h, const SearchParams &P, bool filt, size_t smem_block, int blocks,
+                cudaStream_t s) {
+    return filt ? launch_one<MODE, U8, true>(h, P, smem_block, blocks, s)
+                : launch_one<MODE, U8, false>(h, P, smem_block, blocks, s);
+}
+
+int dispatch(Handle &h, const SearchParams &P, int mode, bool u8, bool filt, size_t smem_block,
+             int blocks, cudaStream_t s) {
+    if (mode == MODE_EXACT)
+        return u8 ? launch_mode<MODE_EXACT, true>(h, P, filt, smem_block, blocks, s)
+                  : launch_mode<MODE_EXACT, false>(h, P, filt, smem_block, blocks, s);
+    return u8 ? launch_mode<MODE_F64, true>(h, P, filt, smem_block, blocks, s)
+              : launch_mode<MODE_F64, false>(h, P, filt, smem_block, blocks, s);
+}
+
+template <int MODE, bool U8, bool FILT>
+int occupancy_of(size_t smem_block, int *blocks_per_sm) {
+    auto kern = search_kernel<MODE, U8, FILT>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem_block)));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, WPB * 32,
+                                                           smem_block));
+    return 0;
+}
+
+int occupancy(int mode, bool u8, bool filt, size_t smem_block, int *bps) {
+    if (mode == MODE_EXACT) {
+        if (u8) return filt ? occupancy_of<1, true, true>(smem_block, bps)
+                            : occupancy_of<1, true, false>(smem_block, bps);
+        return filt ? occupancy_of<1, false, true>(smem_block, bps)
+                    : occupancy_of<1, false, false>(smem_block, bps);
+    }
+    if (u8) return filt ? occupancy_of<0, true, true>(smem_block, bps)
+                        : occupancy_of<0, true, false>(smem_block, bps);
+    return filt ? occupancy_of<0, false, true>(smem_block, bps)
+                : occupancy_of<0, false, false>(smem_block, bps);
+}
+
+int ilog2_ceil(int64_t x) {
+    int l = 0;
+    while ((int64_t(1) << l) < x) l++;
+    return l;
+}
+
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+const char *hnsw_b200_last_error(void) { return hb::g_err.c_str(); }
+
+const char *hnsw_b200_version(void) { return "hnsw_b200 0.1 sm_100a"; }
+
+int hnsw_b200_open(const hnsw_b200_graph_t *graph, void **handle) {
+    if (!graph || !handle) return fail(HNSW_B200_EINVAL, "null argument");
+    const hnsw_b200_graph_t &g = *graph;
+    if (g.n <= 0 || g.n > 0x7ffffffe) return fail(HNSW_B200_EINVAL, "n must be in [1, 2^31 - 2]");
+    if (g.dim <= 0) return fail(HNSW_B200_EINVAL, "dim must be positive");
+    if (!g.vectors || !g.links0 || !g.count0 || !g.upper_offset)
+        return fail(HNSW_B200_EINVAL, "graph arrays must be device pointers");
+    if (g.metric < 0 || g.metric > 2) return fail(HNSW_B200_EINVAL, "unknown metric code");
+    if (g.entry_point < 0 || g.entry_point >= g.n)
+        return fail(HNSW_B200_EINVAL, "entry point outside the graph");
+    if (g.max_level > 0 && (!g.links_up || !g.count_up || g.rows <= 0))
+        return fail(HNSW_B200_EINVAL, "upper layers need links_up and count_up");
+    Handle *h = new Handle();
+    h->g = g;
+    cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (cudaMallocHost(reinterpret_cast<void **>(&h->host_pinned), 4 * sizeof(int32_t)) !=
+        cudaSuccess) {
+        delete h;
+        return fail(HNSW_B200_ENOMEM, "pinned host allocation failed");
+    }
+    *handle = h;
+    return 0;
+}
+
+void hnsw_b200_close(void *handle) {
+    if (!handle) return;
+    Handle *h = static_cast<Handle *>(handle);
+    h->counters.release();
+    h->status.release();
+    h->qlist[0].release();
+    h->qlist[1].release();
+    h->vis.release();
+    h->ties.release();
+    h->spill_d.release();
+    h->spill_i.release();
+    if (h->host_pinned) cudaFreeHost(h->host_pinned);
+    delete h;
+}
+
+int64_t hnsw_b200_last_launches(void *handle) {
+    return handle ? static_cast<Handle *>(handle)->launches : 0;
+}
+
+int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *stream) {
+    if (!handle || !a) return fail(HNSW_B200_EINVAL, "null argument");
+    Handle &h = *static_cast<Handle *>(handle);
+    std::lock_guard<std::mutex> lock(h.mu);
+    h.launches = 0;
+    const hnsw_b200_graph_t &g = h.g;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (a->nq < 0 || a->nq > 0x7fffffff) return fail(HNSW_B200_EINVAL, "nq out of range");
+    if (a->nq == 0) return 0;
+    if (a->k < 1 || a->k_search < a->k) return fail(HNSW_B200_EINVAL, "need 1 <= k <= k_search");
+    if (!a->queries || !a->ef || !a->out_ids || !a->out_dists)
+        return fail(HNSW_B200_EINVAL, "queries, ef and outputs must be device pointers");
+    if (a->use_codes && !g.codes) return fail(HNSW_B200_EINVAL, "graph has no codes");
+    if (a->dist_mode != HNSW_B200_DIST_F64 && a->dist_mode != HNSW_B200_DIST_EXACT_F32)
+        return fail(HNSW_B200_EINVAL, "unknown dist_mode");
+    if (a->dist_mode == HNSW_B200_DIST_EXACT_F32 && g.metric == HNSW_B200_COSINE)
+        return fail(HNSW_B200_EINVAL, "exact float32 mode needs integer data (not cosine)");
+    const bool filt = a->allowed != nullptr;
+    const bool u8 = a->use_codes != 0;
+    const int mode = a->dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64;
+    const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
+    const int krr = a->rerank_queries ? a->k : 0;
+    const int s_cap = 256;
+    const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr);
+    const size_t smem_block = wb * WPB;
+    if (smem_block > 227 * 1024)
+        return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory (" +
+                                          std::to_string(smem_block) + " bytes per block)");
+    int bps = 0;
+    if (int rc = occupancy(mode, u8, filt, smem_block, &bps)) return rc;
+    if (bps < 1) return fail(HNSW_B200_EINVAL, "search kernel cannot be resident");
+    const int32_t nq = int32_t(a->nq);
+
+    // Scratch sizing from the expected work per query: visits grow about linearly with ef and
+    // inversely with the share of allowed nodes.
+    const double p = filt ? std::max(double(a->allowed_fraction), 1.0 / double(g.n)) : 1.0;
+    const double est = std::min(double(g.n) + 64.0, (12.0 * ef_cap + 256.0) / p);
+    int vis_log2 = std::max(8, ilog2_ceil(int64_t(2.0 * est)));
+    int vis_up_log2 = 10;
+    int tie_cap = ef_cap + 64;
+    int spill_cap = filt ? int(std::min(double(g.n) + 64.0, est)) : 0;
+
+    if (int rc = h.counters.ensure(4 * sizeof(int32_t))) return rc;
+    if (int rc = h.status.ensure(size_t(nq) * sizeof(int32_t))) return rc;
+    if (int rc = h.qlist[0].ensure(size_t(nq) * sizeof(int32_t))) return rc;
+    if (int rc = h.qlist[1].ensure(size_t(nq) * sizeof(int32_t))) return rc;
+    int32_t *ctr = static_cast<int32_t *>(h.counters.ptr);
+
+    SearchParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.vectors = g.vectors;
+    P.codes = g.codes;
+    P.links0 = g.links0;
+    P.count0 = g.count0;
+    P.upper_offset = g.upper_offset;
+    P.links_up = g.links_up;
+    P.count_up = g.count_up;
+    P.n = g.n;
+    P.dim = g.dim;
+    P.links0_stride = g.links0_stride;
+    P.links_up_stride = g.links_up_stride;
+    P.metric = g.metric;
+    P.entry_point = g.entry_point;
+    P.max_level = g.max_level;
+    P.queries = a->queries;
+    P.queries_f64 = a->queries_f64;
+    P.k = a->k;
+    P.k_search = a->k_search;
+    P.ef = a->ef;
+    P.ef_cap = ef_cap;
+    P.allowed = a->allowed;
+    P.rerank_queries = a->rerank_queries;
+    P.out_ids = a->out_ids;
+    P.out_dists = a->out_dists;
+    P.out_ctr = a->out_counters;
+    P.status = static_cast<int32_t *>(h.status.ptr);
+    P.queue = ctr;
+    P.n_failed = ctr + 1;
+    P.s_cap = s_cap;
+
+    int32_t n_work = nq;
+    const int32_t *qlist = nullptr;
+    for (int attempt = 0; attempt < 6; attempt++) {
+        const int blocks = int(std::min<int64_t>(int64_t(h.sms) * bps, (n_work + WPB - 1) / WPB));
+        const int64_t slots = int64_t(blocks) * WPB;
+        const int64_t vis_stride = int64_t(1) << std::max(vis_log2, vis_up_log2);
+        if (int rc = h.vis.ensure(size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
+        if (int rc = h.ties.ensure(size_t(slots) * tie_cap * sizeof(int32_t))) return rc;
+        if (filt) {
+            if (int rc = h.spill_d.ensure(size_t(slots) * spill_cap * sizeof(double))) return rc;
+            if (int rc = h.spill_i.ensure(size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
+        }
+        P.vis = static_cast<int32_t *>(h.vis.ptr);
+        P.vis_stride = vis_stride;
+        P.vis_log2 = vis_log2;
+        P.vis_up_log2 = vis_up_log2;
+        P.ties = static_cast<int32_t *>(h.ties.ptr);
+        P.tie_cap = tie_cap;
+        P.spill_d = static_cast<double *>(h.spill_d.ptr);
+        P.spill_i = static_cast<int32_t *>(h.spill_i.ptr);
+        P.spill_cap = spill_cap;
+        P.qlist = qlist;
+        P.n_work = n_work;
+        CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(int32_t), s));
+        if (int rc = dispatch(h, P, mode, u8, filt, smem_block, blocks, s)) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h.host_pinned, ctr, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        const int32_t failed = h.host_pinned[1];
+        if (failed == 0) return 0;
+        // Re-run the overflowed queries with four times the scratch of every kind.
+        int32_t *list = static_cast<int32_t *>(h.qlist[attempt & 1].ptr);
+        CUDA_TRY(cudaMemsetAsync(ctr + 2, 0, sizeof(int32_t), s));
+        collect_failed<<<std::max(1, std::min(1024, (n_work + 255) / 256)), 256, 0, s>>>(
+            P.status, qlist, n_work, list, ctr + 2);
+        CUDA_TRY(cudaGetLastError());
+        h.launches++;
+        CUDA_TRY(cudaStreamSynchronize(s));
+        n_work = failed;
+        qlist = list;
+        vis_log2 = std::min(vis_log2 + 2, ilog2_ceil(2 * g.n + 64));
+        vis_up_log2 = std::min(vis_up_log2 + 2, ilog2_ceil(2 * g.n + 64));
+        vis_log2 = std::max(vis_log2, 8);
+        vis_up_log2 = std::max(vis_up_log2, 8);
+        tie_cap *= 4;
+        if (filt) spill_cap = int(std::min<int64_t>(int64_t(spill_cap) * 4, g.n + 64));
+    }
+    return fail(HNSW_B200_ERETRY, "queries still overflowed scratch after retries");
+}
+
+}  // extern "C"

@@ -1,0 +1,251 @@
+"""The GPU engine: the reference's native graph arrays resident in HBM, searched through the C ABI.
+
+:class:`DeviceGraph` uploads the seven native arrays (``src/hnsw_engine/numba_engine.py:36-44``)
+unchanged -- the device copies are byte-identical to the ``.npy`` files -- and opens a
+``libhnsw_b200`` handle over them. Torch is used only for device memory and streams; every search
+is one call into the library, whose kernels do all the work.
+
+The distance arithmetic of a call is chosen per batch (:func:`DeviceGraph.exact_f32_ok`): when data
+and queries are integer-valued and every partial sum of the distance stays below 2**24, float32
+arithmetic is exact in any order and reproduces the reference's float64 value bit for bit, so the
+fast warp-parallel float32 kernel runs; otherwise the kernel accumulates in float64 sequentially
+over the dimensions, which is the reference's own arithmetic (``_distance``, numba_engine.py:57-70).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Any
+
+import numpy as np
+import torch
+from numpy.typing import NDArray
+
+from . import _lib
+
+EXACT_LIMIT = float(2**24)
+
+
+def _dev_ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else int(t.data_ptr())
+
+
+def pack_mask(mask: NDArray[np.bool_]) -> NDArray[np.uint32]:
+    """Bool mask -> little-endian bitmap words (bit i of word w is node 32 w + i)."""
+    n = mask.shape[0]
+    words = (n + 31) // 32
+    packed = np.packbits(np.ascontiguousarray(mask, dtype=np.bool_), bitorder="little")
+    padded = np.zeros(words * 4, dtype=np.uint8)
+    padded[: packed.shape[0]] = packed
+    return padded.view(np.uint32)
+
+
+def to_device(a: Any, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
+    """Host array or device tensor -> contiguous device tensor of ``dtype`` (H2D copy if host)."""
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    arr = np.ascontiguousarray(a)
+    t = torch.from_numpy(arr)
+    if t.dtype != dtype:
+        t = t.to(dtype)
+    return t.to(device, non_blocking=False).contiguous()
+
+
+class DeviceGraph:
+    """A reference-built HNSW graph resident on one GPU, plus its library handle."""
+
+    def __init__(
+        self,
+        arrays: dict[str, NDArray[Any]],
+        entry_point: int,
+        max_level: int,
+        metric: str,
+        device: str | torch.device = "cuda",
+    ) -> None:
+        self.lib = _lib.load()
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("the B200 engine needs a CUDA device")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.metric = metric
+        self.n, self.dim = arrays["vectors"].shape
+        self.entry_point = int(entry_point)
+        self.max_level = int(max_level)
+        host_vectors = np.ascontiguousarray(arrays["vectors"], dtype=np.float32)
+        self.host_vectors = host_vectors
+        with torch.cuda.device(self.device):
+            self.vectors = to_device(host_vectors, torch.float32, self.device)
+            self.links0 = to_device(arrays["links0"], torch.int32, self.device)
+            self.count0 = to_device(arrays["count0"], torch.int32, self.device)
+            self.upper_offset = to_device(arrays["upper_offset"], torch.int64, self.device)
+            links_up = np.asarray(arrays["links_up"])
+            count_up = np.asarray(arrays["count_up"])
+            self.rows = int(links_up.shape[0])
+            self.links_up_stride = int(links_up.shape[1]) if links_up.ndim == 2 else 1
+            if self.rows == 0:  # keep valid (unused) pointers
+                links_up = np.zeros((1, self.links_up_stride), dtype=np.int32)
+                count_up = np.zeros(1, dtype=np.int32)
+            self.links_up = to_device(links_up, torch.int32, self.device)
+            self.count_up = to_device(count_up, torch.int32, self.device)
+        self.links0_stride = int(arrays["links0"].shape[1])
+        self.codes: torch.Tensor | None = None
+        # Host facts for choosing the exact float32 kernel.
+        self._integer = bool(np.array_equal(host_vectors, np.rint(host_vectors)))
+        self._lo = host_vectors.min(axis=0).astype(np.float64) if self.n else np.zeros(self.dim)
+        self._hi = host_vectors.max(axis=0).astype(np.float64) if self.n else np.zeros(self.dim)
+        self._handle = ctypes.c_void_p()
+        self._open()
+
+    def _graph_struct(self) -> _lib.Graph:
+        return _lib.Graph(
+            vectors=_dev_ptr(self.vectors),
+            codes=_dev_ptr(self.codes),
+            links0=_dev_ptr(self.links0),
+            count0=_dev_ptr(self.count0),
+            upper_offset=_dev_ptr(self.upper_offset),
+            links_up=_dev_ptr(self.links_up),
+            count_up=_dev_ptr(self.count_up),
+            n=self.n,
+            rows=self.rows,
+            dim=self.dim,
+            links0_stride=self.links0_stride,
+            links_up_stride=self.links_up_stride,
+            metric=_lib.METRIC_CODES[self.metric],
+            entry_point=self.entry_point,
+            max_level=self.max_level,
+            reserved=0,
+        )
+
+    def _open(self) -> None:
+        if self._handle:
+            self.lib.hnsw_b200_close(self._handle)
+            self._handle = ctypes.c_void_p()
+        g = self._graph_struct()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.hnsw_b200_open(ctypes.byref(g), ctypes.byref(self._handle)))
+
+    def attach_codes(self, codes: NDArray[np.uint8]) -> None:
+        """Upload scalar-quantizer codes (n, dim) uint8 for code-space searches."""
+        if codes.shape != (self.n, self.dim) or codes.dtype != np.uint8:
+            raise ValueError(f"codes must be uint8 with shape {(self.n, self.dim)}")
+        with torch.cuda.device(self.device):
+            self.codes = to_device(codes, torch.uint8, self.device)
+        self._open()
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            self.lib.hnsw_b200_close(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter teardown order varies
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def last_launches(self) -> int:
+        return int(self.lib.hnsw_b200_last_launches(self._handle))
+
+    # ------------------------------------------------------------------ arithmetic selection
+    def exact_f32_ok(self, queries: NDArray[Any], codes: bool, step_lo_hi=None) -> bool:
+        """Whether float32 arithmetic is exact for this batch (integer data, partial sums < 2**24)."""
+        if self.metric == "cosine":
+            return False
+        if codes:
+            lo, hi = np.zeros(self.dim), np.full(self.dim, 255.0)
+        else:
+            if not self._integer:
+                return False
+            lo, hi = self._lo, self._hi
+        q = np.asarray(queries, dtype=np.float64)
+        if q.size == 0:
+            return True
+        if not np.array_equal(q, np.rint(q)):
+            return False
+        if self.metric == "l2":
+            span = np.maximum(np.abs(q - lo), np.abs(hi - q))
+            bound = (span * span).sum(axis=1).max()
+        else:
+            bound = (np.abs(q) * np.maximum(np.abs(lo), np.abs(hi))).sum(axis=1).max()
+        return bool(bound < EXACT_LIMIT)
+
+    # ------------------------------------------------------------------------------ search
+    def search(
+        self,
+        queries: Any,
+        k: int,
+        ef: Any,
+        *,
+        allowed: NDArray[np.bool_] | torch.Tensor | None = None,
+        allowed_fraction: float | None = None,
+        use_codes: bool = False,
+        k_search: int | None = None,
+        rerank_queries: Any = None,
+        dist_mode: int | None = None,
+        counters: bool = True,
+        out: tuple[torch.Tensor, ...] | None = None,
+    ) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor | None]:
+        """One batched search; returns device tensors ``(ids, dists, counters)``.
+
+        ``queries``: (nq, dim) float32 prepared queries, or float64 code-space queries with
+        ``use_codes``. ``ef``: scalar or (nq,) raw efSearch (layer 0 uses ``max(ef, k_search)``).
+        ``allowed``: bool mask (n,) or a device uint32 bitmap. ``rerank_queries``: float32 prepared
+        queries for the fused exact re-rank of the first ``k_search`` beam entries.
+        """
+        dev = self.device
+        nq = int(queries.shape[0])
+        ks = int(k if k_search is None else k_search)
+        q_f64 = use_codes
+        if dist_mode is None:
+            host_q = queries.detach().cpu().numpy() if isinstance(queries, torch.Tensor) else queries
+            dist_mode = _lib.DIST_EXACT_F32 if self.exact_f32_ok(host_q, use_codes) else _lib.DIST_F64
+        with torch.cuda.device(dev):
+            q = to_device(queries, torch.float64 if q_f64 else torch.float32, dev)
+            if isinstance(ef, torch.Tensor):
+                ef_t = ef.to(device=dev, dtype=torch.int32).contiguous()
+                ef_max = int(ef_t.max().item()) if nq else 1
+            else:
+                ef_arr = np.broadcast_to(np.asarray(ef, dtype=np.int32), (nq,))
+                ef_max = int(ef_arr.max()) if nq else 1
+                ef_t = to_device(np.ascontiguousarray(ef_arr), torch.int32, dev)
+            bitmap = None
+            frac = 1.0
+            if allowed is not None:
+                if isinstance(allowed, torch.Tensor) and allowed.dtype == torch.int32:
+                    bitmap = allowed.contiguous()
+                    frac = 1.0 if allowed_fraction is None else float(allowed_fraction)
+                else:
+                    mask = np.asarray(allowed.cpu() if isinstance(allowed, torch.Tensor) else allowed)
+                    frac = float(mask.mean()) if mask.size else 1.0
+                    bitmap = to_device(pack_mask(mask).view(np.int32), torch.int32, dev)
+            rq = None
+            if rerank_queries is not None:
+                rq = to_device(rerank_queries, torch.float32, dev)
+            if out is None:
+                ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
+                dists = torch.empty((nq, k), dtype=torch.float64, device=dev)
+                ctr = torch.empty((nq, 2), dtype=torch.int64, device=dev) if counters else None
+            else:
+                ids, dists, ctr = out
+            args = _lib.SearchArgs(
+                queries=_dev_ptr(q),
+                queries_f64=int(q_f64),
+                use_codes=int(use_codes),
+                nq=nq,
+                k=int(k),
+                k_search=ks,
+                ef=_dev_ptr(ef_t),
+                ef_max=max(ef_max, ks),
+                dist_mode=int(dist_mode),
+                allowed=_dev_ptr(bitmap),
+                allowed_fraction=frac,
+                rerank_queries=_dev_ptr(rq),
+                out_ids=_dev_ptr(ids),
+                out_dists=_dev_ptr(dists),
+                out_counters=_dev_ptr(ctr),
+            )
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args), ctypes.c_void_p(stream)))
+        return ids, dists, ctr

@@ -1,0 +1,398 @@
+"""Search-side drop-in for the reference's ``HNSWIndex`` (``src/hnsw_engine/index.py:96-466``).
+
+The index opens a graph written by the reference's ``save_native`` (``index.py:390-425``,
+``persistence.py:192-243``) and searches it on the GPU with exactly the reference's results. The
+public search surface keeps the reference's names, defaults, argument meaning, validation and
+error messages:
+
+* ``search(query, k=10, ef=None, filter=None)`` and ``batch_search(queries, k=10, ef=None,
+  filter=None)`` (``index.py:244-292``), with ``ef <- max(ef or ef_search, k)`` and an all-false
+  filter returning padding without searching (``:289-291``);
+* cumulative ``distance_computations`` / ``hops`` counters, ``stats()`` and ``reset_counters()``
+  (``:329-365``) with the reference's definitions;
+* extension: ``ef`` may also be an integer array with one efSearch per query, and inputs may be
+  torch device tensors (``batch_search`` then returns device tensors).
+
+Graph construction is not part of this engine: graphs are built by the reference host build, whose
+sequential insertion defines them, and ``add`` says so.
+"""
+
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import asdict, dataclass
+from pathlib import Path
+from typing import Any
+
+import numpy as np
+import torch
+from numpy.typing import ArrayLike, NDArray
+
+from .engine import DeviceGraph
+from .validation import (
+    NATIVE_ARRAYS,
+    as_matrix,
+    as_vector,
+    check_int,
+    check_k,
+    check_native_shapes,
+    prepare,
+    validate_metric,
+    validate_native,
+)
+
+NATIVE_FORMAT = "hnsw-engine-native"
+NATIVE_FORMAT_VERSION = 1
+NATIVE_HEADER = "header.json"
+SELECTIONS = ("simple", "heuristic")
+
+
+@dataclass(frozen=True)
+class IndexStats:
+    """Summary of an index, with the fields of the reference's ``IndexStats`` (index.py:63-93)."""
+
+    size: int
+    dim: int
+    metric: str
+    engine: str
+    M: int
+    max_links_layer0: int
+    ef_construction: int
+    ef_search: int
+    m_L: float
+    selection: str
+    extend_candidates: bool
+    keep_pruned_connections: bool
+    max_level: int
+    entry_point: int
+    nodes_per_layer: tuple[int, ...]
+    links_per_layer: tuple[int, ...]
+    mean_degree_per_layer: tuple[float, ...]
+    memory_bytes: int
+    distance_computations: int
+    hops: int
+
+    def as_dict(self) -> dict[str, Any]:
+        return asdict(self)
+
+
+def read_native(directory: str | Path, mmap: bool = True) -> tuple[dict[str, Any], dict[str, NDArray[Any]]]:
+    """Read a ``save_native`` directory; same checks and messages as ``persistence.load_native``."""
+    root = Path(directory)
+    header_path = root / NATIVE_HEADER
+    if not header_path.is_file():
+        raise ValueError(f"{root} is not an hnsw-engine native index (no {NATIVE_HEADER})")
+    meta: dict[str, Any] = json.loads(header_path.read_text())
+    if meta.pop("format", None) != NATIVE_FORMAT:
+        raise ValueError(f"{root} is not an hnsw-engine native index")
+    version = meta.pop("format_version", None)
+    if version != NATIVE_FORMAT_VERSION:
+        raise ValueError(f"unsupported native format version {version!r}")
+    arrays: dict[str, NDArray[Any]] = {}
+    for name, expected in meta.pop("arrays").items():
+        array = np.load(root / f"{name}.npy", mmap_mode="r" if mmap else None, allow_pickle=False)
+        if str(array.dtype) != expected["dtype"] or list(array.shape) != expected["shape"]:
+            raise ValueError(
+                f"{name}.npy has dtype {array.dtype} and shape {array.shape}, header says "
+                f"{expected['dtype']} and {tuple(expected['shape'])}"
+            )
+        arrays[name] = np.asarray(array)
+    return meta, arrays
+
+
+class HNSWIndex:
+    """An HNSW graph built by the reference, searched on one B200.
+
+    Open one with :meth:`load_native` (a ``save_native`` directory) or :meth:`from_arrays`.
+    Constructor parameters mirror the reference's (``index.py:115-149``); only ``ef_search`` and
+    ``metric`` affect searching.
+    """
+
+    def __init__(
+        self,
+        dim: int,
+        metric: str = "l2",
+        M: int = 16,
+        ef_construction: int = 200,
+        ef_search: int = 50,
+        seed: int | None = None,
+        selection: str = "heuristic",
+        extend_candidates: bool = False,
+        keep_pruned_connections: bool = False,
+        m_L: float | None = None,
+        engine: str = "b200",
+        device: str | torch.device = "cuda",
+    ) -> None:
+        self._dim = check_int(dim, "dim", minimum=1)
+        self._metric = validate_metric(metric)
+        self._M = check_int(M, "M", minimum=2)
+        self._ef_construction = check_int(ef_construction, "ef_construction", minimum=1)
+        self._ef_search = check_int(ef_search, "ef_search", minimum=1)
+        self._seed = None if seed is None else check_int(seed, "seed", minimum=0)
+        if selection not in SELECTIONS:
+            raise ValueError(f"unknown selection {selection!r}; expected one of {SELECTIONS}")
+        self._selection = selection
+        self._extend_candidates = bool(extend_candidates)
+        self._keep_pruned = bool(keep_pruned_connections)
+        self._m_L = 1.0 / math.log(self._M) if m_L is None else float(m_L)
+        self._engine_name = engine
+        self._device = device
+        self._graph: DeviceGraph | None = None
+        self._arrays: dict[str, NDArray[Any]] | None = None
+        self._size = 0
+        self._counters = np.zeros(2, dtype=np.int64)  # distance computations, hops
+        self._meta_extra: dict[str, Any] = {}
+
+    # ----------------------------------------------------------------------- opening
+    @classmethod
+    def load_native(
+        cls, directory: str | Path, mmap: bool = True, validate: bool = True,
+        device: str | torch.device = "cuda",
+    ) -> HNSWIndex:
+        """Open a directory written by the reference's ``HNSWIndex.save_native``."""
+        meta, arrays = read_native(directory, mmap=mmap)
+        params = {k: v for k, v in meta["params"].items() if k != "engine"}
+        index = cls(**params, device=device)
+        index._meta_extra = {"rng_state": meta.get("rng_state")}
+        index._attach(arrays, int(meta["entry_point"]), int(meta["max_level"]), validate)
+        return index
+
+    @classmethod
+    def from_arrays(
+        cls, arrays: dict[str, NDArray[Any]], entry_point: int, max_level: int, *, validate: bool = True,
+        **params: Any,
+    ) -> HNSWIndex:
+        """Wrap native arrays (``NumbaEngine.native_arrays()`` layout) already in memory."""
+        index = cls(**params)
+        index._attach(arrays, int(entry_point), int(max_level), validate)
+        return index
+
+    def _attach(self, arrays: dict[str, NDArray[Any]], entry_point: int, max_level: int,
+                validate: bool) -> None:
+        check_native_shapes(arrays, self._dim, self._M)
+        if validate:
+            validate_native(arrays, entry_point, max_level, self._M)
+        self._arrays = {name: arrays[name] for name in NATIVE_ARRAYS}
+        self._size = int(arrays["vectors"].shape[0])
+        self._entry_point = entry_point
+        self._max_level = max_level
+        if self._size:
+            self._graph = DeviceGraph(self._arrays, entry_point, max_level, self._metric, self._device)
+
+    # ---------------------------------------------------------------------- properties
+    @property
+    def dim(self) -> int:
+        return self._dim
+
+    @property
+    def metric(self) -> str:
+        return self._metric
+
+    @property
+    def M(self) -> int:
+        return self._M
+
+    @property
+    def ef_search(self) -> int:
+        return self._ef_search
+
+    @ef_search.setter
+    def ef_search(self, value: int) -> None:
+        self._ef_search = check_int(value, "ef_search", minimum=1)
+
+    @property
+    def engine(self) -> str:
+        return self._engine_name
+
+    @property
+    def entry_point(self) -> int:
+        return self._entry_point if self._size else -1
+
+    @property
+    def max_level(self) -> int:
+        return self._max_level if self._size else -1
+
+    @property
+    def device_graph(self) -> DeviceGraph:
+        if self._graph is None:
+            raise ValueError("cannot search an empty index")
+        return self._graph
+
+    @property
+    def distance_computations(self) -> int:
+        return int(self._counters[0])
+
+    @property
+    def hops(self) -> int:
+        return int(self._counters[1])
+
+    def native_arrays(self) -> dict[str, NDArray[Any]]:
+        if self._arrays is None:
+            raise ValueError("the index holds no graph")
+        return self._arrays
+
+    def __len__(self) -> int:
+        return self._size
+
+    def __repr__(self) -> str:
+        return (
+            f"HNSWIndex(dim={self._dim}, metric={self._metric!r}, M={self._M}, "
+            f"ef_search={self._ef_search}, engine={self._engine_name!r}, size={len(self)})"
+        )
+
+    # -------------------------------------------------------------------- construction
+    def add(self, vectors: ArrayLike) -> NDArray[np.int64]:
+        raise NotImplementedError(
+            "graph construction stays on the reference host build (hnsw_engine.HNSWIndex.add, "
+            "then save_native); open the result with HNSWIndex.load_native"
+        )
+
+    # --------------------------------------------------------------------------- search
+    def _prepare(self, vectors: ArrayLike) -> NDArray[np.float32]:
+        return prepare(as_matrix(vectors, "vectors", dim=self._dim), self._metric)
+
+    def _check_search_args(self, k: int, ef: Any) -> tuple[int, Any]:
+        if len(self) == 0:
+            raise ValueError("cannot search an empty index")
+        k_valid = check_k(k, len(self))
+        if ef is None:
+            return k_valid, max(self._ef_search, k_valid)
+        if isinstance(ef, (np.ndarray, torch.Tensor, list, tuple)):
+            arr = np.asarray(ef.cpu() if isinstance(ef, torch.Tensor) else ef)
+            if arr.ndim != 1 or not np.issubdtype(arr.dtype, np.integer):
+                raise TypeError("ef must be an integer or a 1-D integer array (one per query)")
+            if arr.size and arr.min() < 1:
+                raise ValueError(f"ef must be >= 1, got {int(arr.min())}")
+            return k_valid, np.maximum(arr.astype(np.int32), k_valid)
+        return k_valid, max(check_int(ef, "ef", minimum=1), k_valid)
+
+    def _check_filter(self, filter: ArrayLike | None) -> NDArray[np.bool_] | None:
+        if filter is None:
+            return None
+        mask = np.asarray(filter.cpu() if isinstance(filter, torch.Tensor) else filter)
+        if mask.dtype != np.bool_:
+            raise TypeError(f"filter must be a boolean array, got dtype {mask.dtype}")
+        if mask.shape != (len(self),):
+            raise ValueError(
+                f"filter must have one entry per indexed vector ({len(self)}), got shape "
+                f"{mask.shape}"
+            )
+        return np.ascontiguousarray(mask)
+
+    def search(
+        self, query: ArrayLike, k: int = 10, ef: int | None = None, filter: ArrayLike | None = None
+    ) -> tuple[NDArray[np.int64], NDArray[np.float64]]:
+        """Approximate ``k`` nearest neighbours of one ``(dim,)`` query (reference ``index.py:244-273``)."""
+        k_valid, ef_valid = self._check_search_args(k, ef)
+        allowed = self._check_filter(filter)
+        prepared = self._prepare(as_vector(query, "query", dim=self._dim)[None, :])
+        if allowed is not None and not allowed.any():
+            return np.full(k_valid, -1, dtype=np.int64), np.full(k_valid, np.inf)
+        ids, dists = self._run(prepared, k_valid, ef_valid, allowed)
+        return ids[0], dists[0]
+
+    def batch_search(
+        self, queries: Any, k: int = 10, ef: Any = None, filter: ArrayLike | None = None
+    ) -> tuple[Any, Any]:
+        """:meth:`search` for each row of ``(nq, dim)`` queries (reference ``index.py:275-292``).
+
+        ``ef`` may be one integer or an array of one efSearch per query. Torch device queries give
+        device results (no host round trip); host queries give numpy results.
+        """
+        k_valid, ef_valid = self._check_search_args(k, ef)
+        allowed = self._check_filter(filter)
+        on_device = isinstance(queries, torch.Tensor) and queries.is_cuda
+        if on_device:
+            if queries.ndim != 2 or queries.shape[1] != self._dim:
+                raise ValueError(f"queries must have shape (nq, {self._dim})")
+            prepared: Any = queries.to(torch.float32)
+            if self._metric == "cosine":
+                q64 = queries.to(torch.float64)
+                prepared = (q64 / torch.linalg.norm(q64, dim=1, keepdim=True)).to(torch.float32)
+        else:
+            prepared = self._prepare(queries)
+        nq = prepared.shape[0]
+        if allowed is not None and not allowed.any():
+            ids = np.full((nq, k_valid), -1, dtype=np.int64)
+            dists = np.full((nq, k_valid), np.inf)
+            if on_device:
+                return torch.from_numpy(ids).to(queries.device), torch.from_numpy(dists).to(queries.device)
+            return ids, dists
+        ids_t, dists_t = self._run(prepared, k_valid, ef_valid, allowed, keep_device=on_device)
+        return ids_t, dists_t
+
+    def _run(self, prepared: Any, k: int, ef: Any, allowed: NDArray[np.bool_] | None,
+             keep_device: bool = False) -> tuple[Any, Any]:
+        g = self.device_graph
+        ids, dists, ctr = g.search(prepared, k, ef, allowed=allowed)
+        self._accumulate(ctr)
+        if keep_device:
+            return ids, dists
+        return ids.cpu().numpy(), dists.cpu().numpy()
+
+    def _accumulate(self, ctr: torch.Tensor | None) -> None:
+        if ctr is not None and ctr.numel():
+            self._counters += ctr.sum(dim=0).cpu().numpy()
+
+    # ----------------------------------------------------------------------- inspection
+    def stats(self) -> IndexStats:
+        """Sizes, layer structure, degrees, memory estimate and cumulative counters (index.py:329-360)."""
+        arrays = self._arrays
+        if arrays is None or self._size == 0:
+            nodes: tuple[int, ...] = ()
+            links: tuple[int, ...] = ()
+        else:
+            levels = arrays["levels"]
+            top = int(levels.max())
+            nodes = tuple(int((levels >= layer).sum()) for layer in range(top + 1))
+            link_counts = [int(arrays["count0"].sum())]
+            if top > 0:
+                upper = np.flatnonzero(levels > 0)
+                offs = arrays["upper_offset"][upper]
+                lv = levels[upper]
+                for layer in range(1, top + 1):
+                    sel = lv >= layer
+                    link_counts.append(int(arrays["count_up"][offs[sel] + layer - 1].sum()))
+            links = tuple(link_counts)
+        degrees = tuple(lk / nd if nd else 0.0 for lk, nd in zip(links, nodes, strict=True))
+        slots = sum(nd * ((2 * self._M if layer == 0 else self._M) + 1) for layer, nd in enumerate(nodes))
+        memory = self._size * self._dim * 4 + slots * 4 + self._size * 4
+        return IndexStats(
+            size=self._size, dim=self._dim, metric=self._metric, engine=self._engine_name, M=self._M,
+            max_links_layer0=2 * self._M, ef_construction=self._ef_construction,
+            ef_search=self._ef_search, m_L=self._m_L, selection=self._selection,
+            extend_candidates=self._extend_candidates, keep_pruned_connections=self._keep_pruned,
+            max_level=self.max_level, entry_point=self.entry_point, nodes_per_layer=nodes,
+            links_per_layer=links, mean_degree_per_layer=degrees, memory_bytes=memory,
+            distance_computations=self.distance_computations, hops=self.hops,
+        )
+
+    def reset_counters(self) -> None:
+        self._counters[:] = 0
+
+    def _params(self) -> dict[str, Any]:
+        return {
+            "dim": self._dim, "metric": self._metric, "M": self._M,
+            "ef_construction": self._ef_construction, "ef_search": self._ef_search,
+            "seed": self._seed, "selection": self._selection,
+            "extend_candidates": self._extend_candidates,
+            "keep_pruned_connections": self._keep_pruned, "m_L": self._m_L, "engine": "numba",
+        }
+
+    def save_native(self, directory: str | Path) -> None:
+        """Write the graph back in the reference's native layout (header written last)."""
+        arrays = self.native_arrays()
+        root = Path(directory)
+        root.mkdir(parents=True, exist_ok=True)
+        (root / NATIVE_HEADER).unlink(missing_ok=True)
+        layout = {}
+        for name in NATIVE_ARRAYS:
+            np.save(root / f"{name}.npy", np.ascontiguousarray(arrays[name]), allow_pickle=False)
+            layout[name] = {"dtype": str(arrays[name].dtype), "shape": list(arrays[name].shape)}
+        header = {
+            "format": NATIVE_FORMAT, "format_version": NATIVE_FORMAT_VERSION, "arrays": layout,
+            "params": self._params(), "rng_state": self._meta_extra.get("rng_state"),
+            "entry_point": self.entry_point, "max_level": self.max_level,
+        }
+        (root / NATIVE_HEADER).write_text(json.dumps(header, indent=2))

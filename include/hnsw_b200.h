@@ -1,0 +1,116 @@
+/*
+ * hnsw_b200 -- C ABI of the B200 HNSW query engine (libhnsw_b200.so).
+ *
+ * Plain pointers and sizes only: every array argument is DEVICE memory owned by the caller (the
+ * Python binding passes torch tensors' data pointers); the library owns only its scratch (work
+ * queue, visited tables, candidate spill buffers), allocated on demand and freed by
+ * hnsw_b200_close. Every entry point returns 0 on success or a negative HNSW_B200_E* code, with a
+ * message available from hnsw_b200_last_error() (per calling thread). Nothing is ever trapped on
+ * the device: kernels report capacity overflows per query through a status word and the library
+ * re-runs those queries with larger scratch.
+ *
+ * The entry points replace the reference's compiled search calls (anamankev/hnsw-engine):
+ *   hnsw_b200_open      <- NumbaEngine.attach_native (src/hnsw_engine/numba_engine.py:827-868):
+ *                          borrows the native arrays (already validated by the caller, as
+ *                          _validate_native does at numba_engine.py:878-914).
+ *   hnsw_b200_search    <- NumbaEngine.batch_search / batch_search_codes / rerank
+ *                          (numba_engine.py:652-713) -> _search_batch (:422-503) and
+ *                          _rerank_batch (:506-530), fused into one launch; extended with a
+ *                          per-query ef array and a filter on code-space searches.
+ *   hnsw_b200_exact_knn <- oracle.exact_search (src/hnsw_engine/oracle.py:35-126).
+ *   hnsw_b200_mlp_*     <- no reference counterpart (the learned early-termination network).
+ */
+#ifndef HNSW_B200_H
+#define HNSW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define HNSW_B200_OK 0
+#define HNSW_B200_EINVAL (-1)   /* bad argument */
+#define HNSW_B200_ECUDA (-2)    /* a CUDA runtime call failed */
+#define HNSW_B200_ENOMEM (-3)   /* device allocation failed */
+#define HNSW_B200_ERETRY (-4)   /* queries still overflowed scratch after the maximum retries */
+
+/* Metric codes, as numba_engine._METRIC_CODES (numba_engine.py:32). */
+#define HNSW_B200_L2 0
+#define HNSW_B200_IP 1
+#define HNSW_B200_COSINE 2
+
+/* The reference's native arrays (numba_engine.py:36-44), in device memory, unchanged layout. */
+typedef struct hnsw_b200_graph {
+    const float *vectors;        /* (n, dim) float32, row-major, rows contiguous */
+    const uint8_t *codes;        /* (n, dim) uint8 scalar-quantizer codes, or NULL */
+    const int32_t *links0;       /* (n, links0_stride) int32; first count0[i] valid */
+    const int32_t *count0;       /* (n,) int32 */
+    const int64_t *upper_offset; /* (n,) int64; first links_up row of a node, -1 if level 0 */
+    const int32_t *links_up;     /* (rows, links_up_stride) int32 */
+    const int32_t *count_up;     /* (rows,) int32 */
+    int64_t n;                   /* nodes */
+    int64_t rows;                /* upper-layer rows */
+    int32_t dim;
+    int32_t links0_stride;       /* 2M + 1 */
+    int32_t links_up_stride;     /* M + 1 */
+    int32_t metric;              /* HNSW_B200_L2 / _IP / _COSINE */
+    int64_t entry_point;
+    int32_t max_level;
+    int32_t reserved;
+} hnsw_b200_graph_t;
+
+/* Distance arithmetic of one search call. */
+#define HNSW_B200_DIST_F64 0      /* float64, strictly sequential over dimensions: bit-identical to
+                                     the reference's _distance for any data */
+#define HNSW_B200_DIST_EXACT_F32 1 /* float32 with warp-parallel sums; the caller asserts that data
+                                     and queries are integer-valued with every partial sum below
+                                     2^24, so the result is the same exact integer */
+
+typedef struct hnsw_b200_search_args {
+    const void *queries;          /* (nq, dim): float32, or float64 if queries_f64 */
+    int32_t queries_f64;          /* 1: float64 code-space queries (transform_queries output) */
+    int32_t use_codes;            /* 1: distances to graph->codes instead of graph->vectors */
+    int64_t nq;
+    int32_t k;                    /* results returned per query */
+    int32_t k_search;             /* results collected by the beam (>= k; = fetch when reranking) */
+    const int32_t *ef;            /* (nq,) efSearch per query; layer 0 uses max(ef[i], k_search) */
+    int32_t ef_max;               /* max over ef[] (sizes shared memory) */
+    int32_t dist_mode;            /* HNSW_B200_DIST_* */
+    const uint32_t *allowed;      /* filter bitmap, bit i of word i/32 = node i allowed; NULL = none */
+    float allowed_fraction;       /* share of allowed nodes (sizes scratch); 1 when unfiltered */
+    const float *rerank_queries;  /* (nq, dim) float32 prepared queries: when non-NULL the first
+                                     k_search beam entries are re-scored exactly against
+                                     graph->vectors in float64 and the best k returned */
+    int64_t *out_ids;             /* (nq, k) int64, -1 padded */
+    double *out_dists;            /* (nq, k) float64, +inf padded */
+    int64_t *out_counters;        /* (nq, 2) int64 distance computations, hops; or NULL */
+} hnsw_b200_search_args_t;
+
+/* Create a search handle over a graph whose arrays live on the current CUDA device. */
+int hnsw_b200_open(const hnsw_b200_graph_t *graph, void **handle);
+
+/* Release the handle and its scratch (never the caller's arrays). */
+void hnsw_b200_close(void *handle);
+
+/* Batched search of args->nq queries on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * Synchronises the stream once to read the overflow count, re-running overflowed queries with
+ * larger scratch; results are complete when it returns 0. */
+int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *args, void *stream);
+
+/* Number of device kernel launches made by the last hnsw_b200_search on this handle. */
+int64_t hnsw_b200_last_launches(void *handle);
+
+/* Thread-local text of the last error. */
+const char *hnsw_b200_last_error(void);
+
+/* Library version string. */
+const char *hnsw_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HNSW_B200_H */

@@ -1,0 +1,174 @@
+"""Parity of the CUDA search with the reference: bit-exact ids, distances and work counters.
+
+Every case runs through the C ABI (``libhnsw_b200.so`` via :class:`DeviceGraph` or the
+:class:`HNSWIndex` facade) and is compared with the reference's golden outputs, and on the larger
+graphs with the CPU oracle on the same inputs.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import QUANT_CASES, SEARCH_CASES, case_arrays, iter_search_runs, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _index(arrays, ep, ml, metric, M):
+    from hnsw_engine_b200 import HNSWIndex
+
+    return HNSWIndex.from_arrays(arrays, ep, ml, dim=arrays["vectors"].shape[1], metric=metric, M=M)
+
+
+@pytest.mark.parametrize("name", SEARCH_CASES)
+def test_search_matches_reference_bit_for_bit(name: str) -> None:
+    case = load_golden(f"search_{name}")
+    arrays, ep, ml = case_arrays(case, name)
+    metric = str(case["metric"])
+    M = (arrays["links0"].shape[1] - 1) // 2
+    index = _index(arrays, ep, ml, metric, M)
+    k = int(case["k"])
+    for mi, mask, ef in iter_search_runs(case):
+        index.reset_counters()
+        ids, dists = index.batch_search(case["queries"], k=k, ef=ef, filter=mask)
+        np.testing.assert_array_equal(ids, case[f"ids_m{mi}_ef{ef}"], err_msg=f"{name} m{mi} ef{ef}")
+        np.testing.assert_array_equal(dists, case[f"dists_m{mi}_ef{ef}"])
+        st = index.stats()
+        np.testing.assert_array_equal([st.distance_computations, st.hops], case[f"ctr_m{mi}_ef{ef}"])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_both_arithmetic_modes_agree_on_integer_data(mode: int) -> None:
+    """The float64-sequential kernel and the exact float32 kernel give identical results."""
+    case = load_golden("search_mix10k")
+    arrays, ep, ml = case_arrays(case, "mix10k")
+    index = _index(arrays, ep, ml, "l2", 16)
+    g = index.device_graph
+    q = case["queries"]
+    for ef in (16, 128):
+        ids, dists, ctr = g.search(q, 10, ef, dist_mode=mode)
+        np.testing.assert_array_equal(ids.cpu().numpy(), case[f"ids_m0_ef{ef}"])
+        np.testing.assert_array_equal(dists.cpu().numpy(), case[f"dists_m0_ef{ef}"])
+        np.testing.assert_array_equal(ctr.sum(0).cpu().numpy(), case[f"ctr_m0_ef{ef}"])
+
+
+def test_per_query_ef_matches_grouped_reference_calls() -> None:
+    case = load_golden("search_mix10k")
+    arrays, ep, ml = case_arrays(case, "mix10k")
+    index = _index(arrays, ep, ml, "l2", 16)
+    index.reset_counters()
+    ids, dists = index.batch_search(case["queries"], k=10, ef=case["pq_ef"])
+    np.testing.assert_array_equal(ids, case["pq_ids"])
+    np.testing.assert_array_equal(dists, case["pq_dists"])
+    st = index.stats()
+    np.testing.assert_array_equal([st.distance_computations, st.hops], case["pq_ctr"])
+
+
+@pytest.mark.parametrize("name", QUANT_CASES)
+def test_quantized_search_and_fused_rerank_match_reference(name: str) -> None:
+    from hnsw_engine_b200 import QuantizedIndex
+
+    case = load_golden(f"quant_{name}")
+    arrays, ep, ml = case_arrays(case, name)
+    metric = str(case["metric"])
+    M = (arrays["links0"].shape[1] - 1) // 2
+    qi = QuantizedIndex(_index(arrays, ep, ml, metric, M))
+    for r in case["reranks"]:
+        ids, dists = qi.batch_search(case["queries"], k=int(case["k"]), ef=int(case["ef"]), rerank=int(r))
+        np.testing.assert_array_equal(ids, case[f"ids_r{r}"], err_msg=f"{name} r{r}")
+        np.testing.assert_array_equal(dists, case[f"dists_r{r}"])
+
+
+def test_single_query_search_matches_batch() -> None:
+    case = load_golden("search_cont_l2")
+    arrays, ep, ml = case_arrays(case, "cont_l2")
+    index = _index(arrays, ep, ml, "l2", 8)
+    ids, dists = index.batch_search(case["queries"][:12], k=5, ef=30)
+    for row in range(12):
+        a, b = index.search(case["queries"][row], k=5, ef=30)
+        np.testing.assert_array_equal(a, ids[row])
+        np.testing.assert_array_equal(b, dists[row])
+
+
+def test_all_false_filter_pads_without_searching() -> None:
+    case = load_golden("search_int_l2")
+    arrays, ep, ml = case_arrays(case, "int_l2")
+    index = _index(arrays, ep, ml, "l2", 6)
+    index.reset_counters()
+    ids, dists = index.batch_search(case["queries"][:4], k=3, filter=np.zeros(1500, dtype=bool))
+    assert (ids == -1).all() and np.isinf(dists).all()
+    assert index.stats().distance_computations == 0
+
+
+def test_all_true_filter_takes_the_unfiltered_steps() -> None:
+    case = load_golden("search_cont_l2")
+    arrays, ep, ml = case_arrays(case, "cont_l2")
+    index = _index(arrays, ep, ml, "l2", 8)
+    index.reset_counters()
+    plain = index.batch_search(case["queries"], k=10, ef=30)
+    c_plain = (index.distance_computations, index.hops)
+    index.reset_counters()
+    filt = index.batch_search(case["queries"], k=10, ef=30, filter=np.ones(1500, dtype=bool))
+    for a, b in zip(plain, filt, strict=True):
+        np.testing.assert_array_equal(a, b)
+    assert (index.distance_computations, index.hops) == c_plain
+
+
+def _oracle_compare(arrays, ep, ml, metric, queries, k, ef, mask=None, codes=None):
+    from oracle import cpu
+
+    index = _index(arrays, ep, ml, metric, (arrays["links0"].shape[1] - 1) // 2)
+    g = index.device_graph
+    if codes is not None:
+        g.attach_codes(codes)
+    ids, dists, ctr = g.search(queries, k, ef, allowed=mask, use_codes=codes is not None)
+    o_ids, o_d, o_c = cpu.search_batch(arrays, ep, ml, queries, k, ef, metric, allowed=mask,
+                                       codes=codes, threads=8)
+    np.testing.assert_array_equal(ids.cpu().numpy(), o_ids)
+    np.testing.assert_array_equal(dists.cpu().numpy(), o_d)
+    np.testing.assert_array_equal(ctr.cpu().numpy(), o_c)
+
+
+def _workload(name: str):
+    from hnsw_engine_b200 import graphs
+
+    if not graphs.available(name):
+        pytest.skip(f"graph {name} not built")
+    meta, arrays = graphs.open_workload(name)
+    return arrays, int(meta["entry_point"]), int(meta["max_level"]), meta["params"]["metric"]
+
+
+@pytest.mark.parametrize("name", ["mix100k", "t100k"])
+def test_large_graph_per_query_ef_matches_oracle(name: str) -> None:
+    from hnsw_engine_b200 import graphs, synthetic
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload(name)
+    q = prepare(graphs.workload_queries(name, nq=400), metric)
+    ef = synthetic.per_query_ef(400, seed=5, low=32, high=512)
+    _oracle_compare(arrays, ep, ml, metric, q, 10, ef)
+
+
+@pytest.mark.parametrize("p", [0.5, 0.1, 0.01])
+@pytest.mark.parametrize("kind", ["bernoulli", "prefix"])
+def test_large_graph_filtered_matches_oracle(p: float, kind: str) -> None:
+    from hnsw_engine_b200 import graphs, synthetic
+
+    arrays, ep, ml, metric = _workload("mix100k")
+    n = arrays["vectors"].shape[0]
+    mask = synthetic.bernoulli_mask(n, p) if kind == "bernoulli" else synthetic.prefix_mask(n, p)
+    q = graphs.workload_queries("mix100k", nq=48 if p >= 0.1 else 16)
+    _oracle_compare(arrays, ep, ml, metric, q, 10, 64, mask=mask)
+
+
+def test_large_graph_codes_cosine_match_oracle() -> None:
+    from hnsw_engine_b200 import graphs
+    from hnsw_engine_b200.quantization import ScalarQuantizer
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload("t100k")
+    quant = ScalarQuantizer.fit(arrays["vectors"])
+    codes = quant.encode(arrays["vectors"])
+    q = quant.transform_queries(prepare(graphs.workload_queries("t100k", nq=200), metric), metric)
+    _oracle_compare(arrays, ep, ml, metric, q, 10, 128, codes=codes)
