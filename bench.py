@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the batched HNSW search on one B200 (or N replicas under torchrun).
+
+Workload: the 1M x 128 integer Gaussian-mixture graph (reference host build, M=16,
+efConstruction=200, level seed 42; ``graphs/build_graphs.py``), 10,000 queries from the same
+mixture (seed 1), k=10. A step is one batched search of all queries. Metric: QPS at recall@10 >=
+0.95 (tie-aware recall against the exact oracle): the operating point is the smallest fixed efSearch
+whose recall reaches 0.95 (plain fixed-ef), and, when a trained early-termination network is
+available, the learned-stop search at the same recall target.
+
+``value``: queries/s with queries and graph resident in HBM (device-timed with CUDA events on the
+launching stream, max over ranks). ``e2e``: the same metric through the public API
+(``HNSWIndex.batch_search`` with numpy queries: validation, host->device copy, search,
+device->host copy of ids and distances). ``roofline``: algorithmic bytes per launch (from the
+kernel's own per-query work counters) over the launch duration, against the measured HBM copy
+bandwidth. ``cpu_baseline``: the CPU restatement of the reference search (oracle) on the host's
+cores over a bounded sample of the same queries.
+
+``--impl reference`` times the reference's CPU search path (the C restatement of the reference's
+compiled search, on all host threads) on the same workload and prints the same JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "QPS at recall@10>=0.95, 1M x 128, 1 B200: learned-stop vs plain fixed-ef"
+UNIT = "queries/s"
+RECALL_TARGET = 0.95
+EF_LADDER = (10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512)
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse() -> argparse.Namespace:
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    p.add_argument("--workload", default="mix1m")
+    p.add_argument("--nq", type=int, default=None)
+    p.add_argument("--k", type=int, default=10)
+    p.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------------- helpers
+def dist_env() -> tuple[int, int, int]:
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        d = json.loads(path.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.samples: list[list[str]] = []
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self) -> None:
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits"],
+                    capture_output=True, text=True, timeout=5,
+                ).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self) -> ClockSampler:
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self._stop.set()
+        self._thread.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 5 + i and s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def algorithmic_bytes(counters: np.ndarray, arrays: dict, dim: int, k: int, row_bytes: int) -> float:
+    """Per-launch algorithmic bytes: rows scored, link rows read, queries and results.
+
+    distances x row bytes + hops x (count word + mean used link slots x 4) + nq x (query + k x 16).
+    """
+    dist = float(counters[:, 0].sum())
+    hops = float(counters[:, 1].sum())
+    mean_links = float(np.asarray(arrays["count0"]).mean())
+    nq = counters.shape[0]
+    return dist * row_bytes + hops * (4.0 + 4.0 * mean_links) + nq * (dim * 4.0 + k * 16.0)
+
+
+def ground_truth(vectors_dev, queries: np.ndarray, k: int, metric: str):
+    """Exact top-k (ids, float64 distances) from the tensor-core exact k-NN (untimed)."""
+    import torch
+
+    from hnsw_engine_b200.exact_knn import exact_search
+
+    ids, dists = exact_search(vectors_dev, torch.from_numpy(queries).to(vectors_dev.device), k, metric)
+    return ids.cpu().numpy(), dists.cpu().numpy()
+
+
+def recall_of(ids: np.ndarray, dists: np.ndarray, gt_ids: np.ndarray, gt_d: np.ndarray, k: int) -> float:
+    from hnsw_engine_b200.metrics import recall_at_k
+
+    return recall_at_k(ids, dists, gt_ids, gt_d, k)["recall"]
+
+
+# -------------------------------------------------------------------------------- CPU baselines
+def cpu_sample(arrays, ep, ml, queries, k, ef, metric, seconds: float, threads: int) -> dict:
+    """Time the oracle (C restatement of the reference search) on a bounded sample of queries."""
+    from oracle import cpu
+
+    cpu.build()
+    probe = min(len(queries), max(64, threads * 8))
+    t0 = time.perf_counter()
+    cpu.search_batch(arrays, ep, ml, queries[:probe], k, ef, metric, threads=threads)
+    per_q = (time.perf_counter() - t0) / probe
+    n = int(min(len(queries), max(probe, seconds / max(per_q, 1e-9))))
+    t0 = time.perf_counter()
+    cpu.search_batch(arrays, ep, ml, queries[:n], k, ef, metric, threads=threads)
+    el = time.perf_counter() - t0
+    return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} of {len(queries)} queries at ef={ef if np.isscalar(ef) else 'per-query'}, "
+                      f"C restatement of the reference search (oracle/hnsw_oracle.c), "
+                      f"{threads} threads, {el:.1f} s"}
+
+
+def run_reference(args: argparse.Namespace) -> None:
+    """The reference arm: the reference search path on the host cores, same workload and metric."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from hnsw_engine_b200 import graphs
+    from hnsw_engine_b200.validation import prepare
+    from oracle import cpu
+
+    meta, arrays = graphs.open_workload(args.workload)
+    ep, ml = int(meta["entry_point"]), int(meta["max_level"])
+    metric = meta["params"]["metric"]
+    queries = prepare(graphs.workload_queries(args.workload, nq=args.nq), metric)
+    threads = cpu.default_threads()
+    ef = int(os.environ.get("HNSW_BENCH_EF", "0")) or None
+    if ef is None:
+        op = ROOT / "graphs" / args.workload / "operating_point.json"
+        ef = json.loads(op.read_text())["ef"] if op.is_file() else 32
+    per_step_s = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
+    values = []
+    for step in range(args.warmup + args.steps):
+        res = cpu_sample(arrays, ep, ml, queries, args.k, ef, metric, per_step_s, threads)
+        if step >= args.warmup:
+            values.append(res["value"])
+    value = statistics.median(values)
+    res["value"] = value
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * len(queries) / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{args.workload}: {arrays['vectors'].shape[0]} x {arrays['vectors'].shape[1]} "
+                               f"{metric}, nq={len(queries)}, k={args.k}, ef={ef} (plain fixed-ef operating point)",
+                   "parallelism": "host threads"},
+        "cpu_baseline": res,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------ GPU arm
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from hnsw_engine_b200 import HNSWIndex, graphs
+    from hnsw_engine_b200.validation import prepare
+
+    meta, arrays = graphs.open_workload(args.workload)
+    ep, ml = int(meta["entry_point"]), int(meta["max_level"])
+    params = {k: v for k, v in meta["params"].items() if k != "engine"}
+    metric = params["metric"]
+    index = HNSWIndex.from_arrays(arrays, ep, ml, device=dev, **params)
+    g = index.device_graph
+    raw_q = graphs.workload_queries(args.workload, nq=args.nq)
+    queries = prepare(raw_q, metric)
+    nq, k = queries.shape[0], args.k
+    dim = queries.shape[1]
+
+    # Exact ground truth and the plain fixed-ef operating point.
+    gt_ids, gt_d = ground_truth(g.vectors, queries, k, metric)
+    q_dev = torch.from_numpy(queries).to(dev)
+    sweep = {}
+    ef_op = EF_LADDER[-1]
+    for ef in EF_LADDER:
+        ids, dists, ctr = g.search(q_dev, k, ef)
+        rec = recall_of(ids.cpu().numpy(), dists.cpu().numpy(), gt_ids, gt_d, k)
+        sweep[ef] = rec
+        if rec >= RECALL_TARGET:
+            ef_op = ef
+            break
+    if rank == 0:
+        op_path = ROOT / "graphs" / args.workload / "operating_point.json"
+        try:
+            op_path.write_text(json.dumps({"ef": ef_op, "recall": sweep[ef_op]}))
+        except OSError:
+            pass
+
+    ids_o = torch.empty((nq, k), dtype=torch.int64, device=dev)
+    d_o = torch.empty((nq, k), dtype=torch.float64, device=dev)
+    c_o = torch.empty((nq, 2), dtype=torch.int64, device=dev)
+    mode = 1 if g.exact_f32_ok(queries, False) else 0
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        g.search(q_dev, k, ef_op, out=(ids_o, d_o, c_o), dist_mode=mode)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    launches_per_step = g.last_launches
+    counters = c_o.cpu().numpy()
+    row_bytes = dim * 4
+    alg_bytes = algorithmic_bytes(counters, arrays, dim, k, row_bytes)
+
+    # Device-resident timed region.
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends, strict=True)]
+    total_ms = float(sum(step_ms))
+    if pg is not None:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+        pg.barrier()
+    value = world * nq * args.steps / (total_ms / 1000.0)
+    mean_ms = total_ms / args.steps
+    rec_op = recall_of(ids_o.cpu().numpy(), d_o.cpu().numpy(), gt_ids, gt_d, k)
+
+    # End to end through the public API with host buffers.
+    index.batch_search(raw_q, k=k, ef=ef_op)  # warm
+    torch.cuda.synchronize()
+    e_ms = []
+    for _ in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        e_ids, e_d = index.batch_search(raw_q, k=k, ef=ef_op)
+        torch.cuda.synchronize()
+        e_ms.append((time.perf_counter() - t0) * 1000.0)
+    e2e_ms = float(np.median(e_ms))
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * nq / (e2e_ms / 1000.0)
+    assert np.array_equal(e_ids, ids_o.cpu().numpy()), "e2e results differ from device results"
+
+    # Per-query efSearch uniform on 32..512 (the batched-at-scale configuration).
+    from hnsw_engine_b200 import synthetic
+
+    pq = synthetic.per_query_ef(nq, seed=11, low=32, high=512)
+    pq_dev = torch.from_numpy(pq).to(dev)
+    g.search(q_dev, k, pq_dev, dist_mode=mode)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    pq_ids, pq_d, pq_c = g.search(q_dev, k, pq_dev, dist_mode=mode)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    pq_ms = ev0.elapsed_time(ev1)
+    pq_rec = recall_of(pq_ids.cpu().numpy(), pq_d.cpu().numpy(), gt_ids, gt_d, k)
+    pq_bytes = algorithmic_bytes(pq_c.cpu().numpy(), arrays, dim, k, row_bytes)
+
+    pk = peaks()
+    achieved = alg_bytes / (mean_ms / 1000.0) / 1e9
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import cpu
+
+        cpu_base = cpu_sample(arrays, ep, ml, queries, k, ef_op, metric, args.cpu_sample_seconds,
+                              cpu.default_threads())
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(3, args.warmup),
+            "ms_per_step": mean_ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if mode == 1 else "f64",
+            "data": "synthetic",
+            "config": {
+                "workload": f"{args.workload}: {arrays['vectors'].shape[0]} x {dim} integer mixture, "
+                            f"{metric}, M={params['M']}, efC={params['ef_construction']}, nq={nq}, k={k}",
+                "method": "plain fixed-ef",
+                "ef": ef_op,
+                "recall_at_10": rec_op,
+                "ef_sweep": {str(e): r for e, r in sweep.items()},
+                "l2_policy": "inputs larger than L2 (vectors %d MB + links %d MB > 126 MB)"
+                             % (arrays["vectors"].nbytes >> 20, np.asarray(arrays["links0"]).nbytes >> 20),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "per_query_ef_32_512": {"qps": world * nq / (pq_ms / 1000.0), "recall_at_10": pq_rec,
+                                        "achieved_gbs": pq_bytes / (pq_ms / 1000.0) / 1e9},
+            },
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": pk["hbm_gbs"],
+                "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"],
+                "traffic": None,
+                "peak_source": pk["source"],
+                "algorithmic_bytes_per_launch": alg_bytes,
+            },
+            "cpu_baseline": cpu_base,
+            "e2e": {
+                "value": e2e_value,
+                "unit": UNIT,
+                "h2d_bytes_per_step": int(raw_q.astype(np.float32).nbytes + nq * 4),
+                "d2h_bytes_per_step": int(nq * k * 16 + nq * 16),
+            },
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

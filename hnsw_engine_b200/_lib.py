@@ -65,11 +65,32 @@ class SearchArgs(ctypes.Structure):
     ]
 
 
+class ExactArgs(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("queries", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("dim", ctypes.c_int32),
+        ("n", ctypes.c_int64),
+        ("nq", ctypes.c_int64),
+        ("k", ctypes.c_int32),
+        ("metric", ctypes.c_int32),
+        ("integer_valued", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("out_ids", ctypes.c_void_p),
+        ("out_dists", ctypes.c_void_p),
+        ("out_filter_max_error", ctypes.c_void_p),
+        ("out_candidates", ctypes.c_void_p),
+        ("out_launches", ctypes.c_void_p),
+    ]
+
+
 # Every symbol include/hnsw_b200.h declares, with its ctypes signature.
 SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "hnsw_b200_open": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.POINTER(ctypes.c_void_p)]),
     "hnsw_b200_close": (None, [ctypes.c_void_p]),
     "hnsw_b200_search": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchArgs), ctypes.c_void_p]),
+    "hnsw_b200_exact_knn": (ctypes.c_int, [ctypes.POINTER(ExactArgs), ctypes.c_void_p]),
     "hnsw_b200_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
     "hnsw_b200_last_error": (ctypes.c_char_p, []),
     "hnsw_b200_version": (ctypes.c_char_p, []),

@@ -1,0 +1,815 @@
+// Exact brute-force k-NN on B200 tensor cores (the reference's oracle.exact_search,
+// src/hnsw_engine/oracle.py:35-126, re-designed for sm_100a).
+//
+// Algorithm (the reference's filter-then-rerank, with this kernel's own error bound):
+//  1. prep: rows -> BF16 operands. Integer data with |v| <= 256 is exact in BF16 (one term). Other
+//     data is split v = hi + lo (hi = bf16(v), lo = bf16(v - hi)) and the operands are concatenated
+//     along K as Q' = [q_hi, q_hi, q_lo], X' = [x_hi, x_lo, x_hi], so one GEMM yields
+//     hi.hi + hi.lo + lo.hi (relative error about 2^-16). Norms are computed in float64.
+//  2. filter GEMM (tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in TMEM, TMA-fed, warp specialised):
+//     approx distance a = |q|^2 + |x|^2 - 2 q.x (l2), -q.x (ip) or 1 - q.x (cosine, on float64-
+//     normalised rows); every (query, row) with a <= tau_q + margin_q is appended to the query's
+//     candidate list. margin_q = 2 e_q where e_q bounds |a - exact| for this arithmetic, so every true
+//     top-k row survives whenever tau_q is at least the k-th smallest approximate distance.
+//  3. tau_q: pass one runs the filter on a prefix of the data with tau = +inf, and a radix select
+//     takes the k-th smallest approximate distance of that prefix (an upper bound of the global one).
+//     Pass two filters all rows; a second select tightens tau to the k-th smallest candidate.
+//  4. rerank: float64 distances (sequential over dimensions) of the surviving candidates, best k by
+//     (distance, id) -- ties to the lower id, as np.lexsort((ids, exact)) in the reference.
+// Waits on mbarriers are bounded by a wall-clock limit; on expiry the kernel records an error,
+// drains what it issued and frees its TMEM.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hnsw_b200.h"
+
+namespace hb {
+int fail(int code, const std::string &msg);  // search.cu: records the thread's last error
+}
+
+namespace hbx {
+
+constexpr int BM = 128;  // queries per tile (TMEM lanes)
+constexpr int BN = 256;  // data rows per tile (TMEM columns per accumulator)
+constexpr int BK = 64;   // K elements per stage (128 bytes of BF16: one swizzle-128B row)
+constexpr int STAGES = 4;
+constexpr int A_BYTES = BM * BK * 2;
+constexpr int B_BYTES = BN * BK * 2;
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int FILTER_THREADS = 256;
+constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
+constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s
+
+// UMMA instruction descriptor: BF16 A and B (K-major), FP32 accumulator, M = 128, N = 256.
+constexpr uint32_t IDESC = (1u << 4)            // c_format F32
+                           | (1u << 7)          // a_format BF16
+                           | (1u << 10)         // b_format BF16
+                           | (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+
+struct FilterParams {
+    int32_t nq;            // valid queries
+    int32_t row_begin;     // first data row of this pass
+    int32_t row_end;       // one past the last data row of this pass
+    int32_t kchunks;       // K' / BK
+    int32_t tiles_per_split;
+    int32_t metric;
+    const float *qq;       // |q|^2 per query (l2)
+    const float *xx;       // |x|^2 per row (l2)
+    const float *thr;      // per query: tau + margin (+inf in pass one)
+    float *cand_val;       // (nq, cap) approximate distances
+    int32_t *cand_id;      // (nq, cap) row ids
+    int32_t *cand_cnt;     // (nq,) appended counts (may exceed cap: overflow)
+    int32_t cap;
+    int32_t *err;          // nonzero: a bounded wait expired
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false if the wall-clock limit expired (the caller records the error).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (now_ns() - t0 > WAIT_LIMIT_NS) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *bar, void *dst, int x,
+                                            int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 bytes, 8-row groups
+// 1024 bytes apart (stride byte offset), leading byte offset 16 bytes, descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= uint64_t((saddr >> 4) & 0x3FFF);
+    d |= uint64_t(1) << 16;            // leading byte offset (16 B) >> 4
+    d |= uint64_t(1024 >> 4) << 32;    // stride byte offset >> 4
+    d |= uint64_t(1) << 46;            // version
+    d |= uint64_t(2) << 61;            // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+        "%30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(FILTER_THREADS, 1)
+    knn_filter_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const FilterParams p) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024-byte aligned stage buffers (swizzle-128B atoms), barriers after them.
+    unsigned char *smem = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int qt = blockIdx.x;
+    const int total_tiles = (p.row_end - p.row_begin + BN - 1) / BN;
+    const int t0 = blockIdx.y * p.tiles_per_split;
+    const int t1 = min(total_tiles, t0 + p.tiles_per_split);
+    const int ntiles = max(0, t1 - t0);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(tfull + b, 1);
+            mbar_init(tempty + b, 4);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------------------------------------------------------- TMA producer
+        int it = 0;
+        bool ok = true;
+        for (int lt = 0; lt < ntiles && ok; lt++) {
+            const int row0 = p.row_begin + (t0 + lt) * BN;
+            for (int kc = 0; kc < p.kchunks; kc++, it++) {
+                const int s = it % STAGES;
+                const uint32_t par = ((it / STAGES) & 1) ^ 1;
+                if (!mbar_wait(empty + s, par, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *a = smem + s * STAGE_BYTES;
+                unsigned char *b = a + A_BYTES;
+                mbar_expect_tx(full + s, STAGE_BYTES);
+                tma_load_2d(&tmA, full + s, a, kc * BK, qt * BM);
+                tma_load_2d(&tmB, full + s, b, kc * BK, row0);
+            }
+        }
+        if (!ok) {
+            atomicExch(p.err, 1);
+            *abort_flag = 1;
+        }
+        // Drain: every stage issued must land before the CTA may exit.
+        const int issued = it;
+        for (int j = max(0, issued - STAGES); j < issued; j++) {
+            const int s = j % STAGES;
+            const uint32_t par = (j / STAGES) & 1;
+            const unsigned long long t = now_ns();
+            while (!mbar_try(full + s, par) && now_ns() - t < WAIT_LIMIT_NS) {
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------------------------------------------------------- MMA issuer
+        int it = 0;
+        bool ok = true;
+        for (int lt = 0; lt < ntiles && ok; lt++) {
+            const int b = lt & 1;
+            if (!mbar_wait(tempty + b, ((lt >> 1) & 1) ^ 1, abort_flag)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t tmem_d = tmem_base + uint32_t(b * BN);
+            for (int kc = 0; kc < p.kchunks; kc++, it++) {
+                const int s = it % STAGES;
+                if (!mbar_wait(full + s, (it / STAGES) & 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+                const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+                for (int j = 0; j < BK / 16; j++) {  // K = 16 per instruction, 32 bytes apart
+                    umma_bf16(tmem_d, sw128_desc(a_addr + j * 32), sw128_desc(b_addr + j * 32),
+                              (kc | j) != 0);
+                }
+                umma_commit(empty + s);
+            }
+            if (ok) umma_commit(tfull + b);
+        }
+        if (!ok) {
+            atomicExch(p.err, 1);
+            *abort_flag = 1;
+        }
+        // Every MMA issued must finish before TMEM is released: commit one more arrival on a
+        // stage barrier and wait for it (tcgen05.commit tracks all prior MMAs of this thread).
+        if (it > 0) {
+            const int s = (it - 1) % STAGES;
+            const uint32_t par = ((it - 1) / STAGES) & 1;
+            const unsigned long long t = now_ns();
+            while (!mbar_try(empty + s, par) && now_ns() - t < WAIT_LIMIT_NS) {
+            }
+        }
+    } else if (warp >= 4) {
+        // ---------------------------------------------------------------- epilogue
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;  // TMEM lane = query row of the tile
+        const int q = qt * BM + row;
+        const bool qvalid = q < p.nq;
+        const float qq = qvalid ? p.qq[q] : 0.f;
+        const float thr = qvalid ? p.thr[q] : -INFINITY;
+        float *cv = p.cand_val + int64_t(qvalid ? q : 0) * p.cap;
+        int32_t *ci = p.cand_id + int64_t(qvalid ? q : 0) * p.cap;
+        for (int lt = 0; lt < ntiles; lt++) {
+            const int b = lt & 1;
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait(tfull + b, (lt >> 1) & 1, abort_flag) ? 1 : 0;
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0) {
+                    atomicExch(p.err, 1);
+                    *abort_flag = 1;
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int row0 = p.row_begin + (t0 + lt) * BN;
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 32) {
+                float v[32];
+                tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
+                const int col0 = row0 + c;
+                uint32_t keep = 0;
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const int id = col0 + j;
+                    float a;
+                    if (p.metric == HNSW_B200_L2)
+                        a = fmaf(-2.f, v[j], qq + __ldg(p.xx + min(id, p.row_end - 1)));
+                    else if (p.metric == HNSW_B200_IP)
+                        a = -v[j];
+                    else
+                        a = 1.f - v[j];
+                    v[j] = a;
+                    if (a <= thr && id < p.row_end) keep |= 1u << j;
+                }
+                if (keep && qvalid) {
+                    const int cnt = __popc(keep);
+                    const int base = atomicAdd(p.cand_cnt + q, cnt);
+                    int o = base;
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        if ((keep >> j) & 1u) {
+                            if (o < p.cap) {
+                                cv[o] = v[j];
+                                ci[o] = col0 + j;
+                            }
+                            o++;
+                        }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty + b);
+        }
+    }
+    __syncthreads();
+    if (warp == 2) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(TMEM_COLS));
+    }
+}
+
+// ------------------------------------------------------------------------------------- prep
+// One warp per row: float64 norm, cosine normalisation, BF16 operand row(s) of width kpad.
+// terms == 1: [v]; terms == 3: A-side [hi, hi, lo] (queries) or B-side [hi, lo, hi] (data).
+template <typename T>
+__global__ void prep_rows(const T *src, int64_t rows, int dim, int64_t rows_pad, int kpad,
+                          int terms, int a_side, int cosine, __nv_bfloat16 *dst, double *norm64,
+                          float *sq32) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int seg = kpad / terms;  // padded dim per term
+    for (int64_t r = warp; r < rows_pad; r += nwarps) {
+        __nv_bfloat16 *out = dst + r * kpad;
+        if (r >= rows) {
+            for (int i = lane; i < kpad; i += 32) out[i] = __float2bfloat16(0.f);
+            continue;
+        }
+        const T *x = src + r * dim;
+        double ss = 0.0;
+        for (int i = lane; i < dim; i += 32) {
+            const double v = double(x[i]);
+            ss += v * v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        const double nrm = sqrt(ss);
+        const double scale = cosine ? (nrm > 0 ? 1.0 / nrm : 0.0) : 1.0;
+        for (int i = lane; i < seg; i += 32) {
+            const double v = i < dim ? double(x[i]) * scale : 0.0;
+            const float vf = float(v);
+            const __nv_bfloat16 hi = __float2bfloat16_rn(vf);
+            if (terms == 1) {
+                out[i] = hi;
+            } else {
+                const __nv_bfloat16 lo = __float2bfloat16_rn(float(v - double(__bfloat162float(hi))));
+                out[i] = hi;
+                out[seg + i] = a_side ? hi : lo;
+                out[2 * seg + i] = a_side ? lo : hi;
+            }
+        }
+        if (lane == 0) {
+            norm64[r] = nrm;  // cosine rerank re-normalises with it; margins use 1 for cosine
+            sq32[r] = cosine ? 1.f : float(ss);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ radix select
+// Order-preserving key of a float (ascending floats -> ascending unsigned keys).
+__device__ __forceinline__ uint32_t fkey(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float funkey(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// One block of 256 threads per query: tau[q] = k-th smallest of the candidate values (or +inf if
+// fewer than k), then out_thr[q] = tau + margin[q].
+__global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32_t cap, int32_t nq,
+                           int32_t k, const float *margin, float *out_thr, float *out_tau) {
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t s_prefix, s_rank;
+    const int q = blockIdx.x;
+    if (q >= nq) return;
+    const int m = min(cand_cnt[q], cap);
+    const float *v = cand_val + int64_t(q) * cap;
+    if (m < k) {
+        if (threadIdx.x == 0) {
+            out_tau[q] = INFINITY;
+            out_thr[q] = INFINITY;
+        }
+        return;
+    }
+    uint32_t prefix = 0, rank = uint32_t(k);  // rank: 1-based position within the current bucket
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        const uint32_t hmask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const uint32_t key = fkey(v[i]);
+            if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            int bin = 0;
+            for (; bin < 256; bin++) {
+                if (acc + hist[bin] >= rank) break;
+                acc += hist[bin];
+            }
+            s_prefix = prefix | (uint32_t(bin) << shift);
+            s_rank = rank - acc;
+        }
+        __syncthreads();
+        prefix = s_prefix;
+        rank = s_rank;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float tau = funkey(prefix);
+        out_tau[q] = tau;
+        out_thr[q] = tau + margin[q];
+    }
+}
+
+// ------------------------------------------------------------------------------------ rerank
+__device__ __forceinline__ bool pair_lt(double da, int32_t ia, double db, int32_t ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+// One warp per query: exact float64 distances of the candidates within the final threshold,
+// best k by (distance, id) kept in shared memory (sorted insertion), written as int64 / float64.
+template <typename T>
+__global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq, int32_t k,
+                            int32_t metric, const double *xnorm, const double *qnorm,
+                            const float *cand_val, const int32_t *cand_id, const int32_t *cand_cnt,
+                            int32_t cap, const float *thr, int64_t *out_ids, double *out_d) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int warps = blockDim.x >> 5;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * warps + w;
+    double *Ad = reinterpret_cast<double *>(sm) + size_t(w) * (k + 1);
+    int32_t *Ai = reinterpret_cast<int32_t *>(reinterpret_cast<double *>(sm) + size_t(warps) * (k + 1)) +
+                  size_t(w) * (k + 1);
+    if (q >= nq) return;
+    const int m = min(cand_cnt[q], cap);
+    const float t = thr[q];
+    const T *qv = queries + int64_t(q) * dim;
+    const double qn = qnorm[q];
+    int a = 0;
+    for (int base = 0; base < m; base += 32) {
+        const int i = base + lane;
+        bool has = i < m && cand_val[int64_t(q) * cap + i] <= t;
+        int32_t id = has ? cand_id[int64_t(q) * cap + i] : -1;
+        double d = INFINITY;
+        if (has) {
+            const T *x = data + int64_t(id) * dim;
+            double acc = 0.0;
+            if (metric == HNSW_B200_L2) {
+                for (int j = 0; j < dim; j++) {
+                    const double df = __dsub_rn(double(x[j]), double(qv[j]));
+                    acc = __dadd_rn(acc, __dmul_rn(df, df));
+                }
+                d = acc;
+            } else if (metric == HNSW_B200_IP) {
+                for (int j = 0; j < dim; j++) acc = __dadd_rn(acc, __dmul_rn(double(x[j]), double(qv[j])));
+                d = -acc;
+            } else {
+                const double xn = xnorm[id];
+                for (int j = 0; j < dim; j++)
+                    acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[j]), xn), __ddiv_rn(double(qv[j]), qn)));
+                d = __dsub_rn(1.0, acc);
+            }
+        }
+        uint32_t am = __ballot_sync(0xffffffffu, has);
+        while (am) {
+            const int j = __ffs(am) - 1;
+            am &= am - 1;
+            const double xd = __shfl_sync(0xffffffffu, d, j);
+            const int32_t xi = __shfl_sync(0xffffffffu, id, j);
+            if (a == k && !pair_lt(xd, xi, Ad[k - 1], Ai[k - 1])) continue;
+            int c = 0;
+            for (int r = lane; r < a; r += 32) c += pair_lt(Ad[r], Ai[r], xd, xi);
+            const int pos = __reduce_add_sync(0xffffffffu, c);
+            for (int top = a - 1; top >= pos; top -= 32) {
+                const int r = top - lane;
+                double dv = 0;
+                int32_t iv = 0;
+                if (r >= pos) {
+                    dv = Ad[r];
+                    iv = Ai[r];
+                }
+                __syncwarp();
+                if (r >= pos) {
+                    Ad[r + 1] = dv;
+                    Ai[r + 1] = iv;
+                }
+                __syncwarp();
+            }
+            if (lane == 0) {
+                Ad[pos] = xd;
+                Ai[pos] = xi;
+            }
+            __syncwarp();
+            a = min(a + 1, k);
+        }
+    }
+    for (int r = lane; r < k; r += 32) {
+        out_ids[int64_t(q) * k + r] = r < a ? int64_t(Ai[r]) : -1;
+        out_d[int64_t(q) * k + r] = r < a ? Ad[r] : INFINITY;
+    }
+}
+
+// Error bound of the filter arithmetic and the per-query margins (2 e_q).
+__global__ void margins_kernel(const double *qnorm, int32_t nq, double xmax, int kp, int terms,
+                               int metric, float *margin) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const double qn = metric == HNSW_B200_COSINE ? 1.0 : qnorm[q];
+    const double xm = metric == HNSW_B200_COSINE ? 1.0 : xmax;
+    const double rep = terms == 1 ? 0.0 : ldexp(1.0, -15);          // dropped lo.lo and rounding
+    const double acc = double(kp + 8) * ldexp(1.0, -22);             // FP32 accumulation (2u per add)
+    const double e_dot = (rep + acc) * 1.25 * qn * xm;
+    double e = e_dot;
+    if (metric == HNSW_B200_L2) e = 2.0 * e_dot + ldexp(1.0, -20) * (qn + xm) * (qn + xm);
+    else e = e_dot + ldexp(1.0, -22);
+    margin[q] = float(2.0 * e * 1.0001);
+}
+
+// ============================================================================== host
+using hb::fail;
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+int make_map(CUtensorMap *map, const void *base, int64_t rows, int kpad, int box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return fail(HNSW_B200_ECUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[2] = {cuuint64_t(kpad), cuuint64_t(rows)};
+    cuuint64_t strides[1] = {cuuint64_t(kpad) * 2};
+    cuuint32_t box[2] = {cuuint32_t(BK), cuuint32_t(box_rows)};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(HNSW_B200_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r)));
+    return 0;
+}
+
+struct Scratch {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~Scratch() {
+        if (p) cudaFree(p);
+    }
+    int get(size_t b) {
+        if (b <= bytes) return 0;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (cudaMalloc(&p, b) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HNSW_B200_ENOMEM, "exact knn scratch allocation failed");
+        }
+        bytes = b;
+        return 0;
+    }
+};
+
+#define XT(expr)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (expr);                                                               \
+        if (e_ != cudaSuccess) return fail(HNSW_B200_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <typename T>
+int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
+    const int64_t n = a->n, nq_all = a->nq;
+    const int dim = a->dim, k = a->k, metric = a->metric;
+    const int terms = a->integer_valued && metric != HNSW_B200_COSINE ? 1 : 3;
+    const int seg = (dim + BK - 1) / BK * BK;
+    const int kp = seg * terms;
+    const int64_t n_pad = (n + BN - 1) / BN * BN;
+    const int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
+    const int64_t q_pad = (QB + BM - 1) / BM * BM;
+    const int qtiles = int(q_pad / BM);
+    int sms = 148;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+    // Candidate capacity: pass one keeps every row of its prefix; pass two about k * n / prefix.
+    const int64_t prefix = std::min<int64_t>(n, std::max<int64_t>(int64_t(64) * k, 32768));
+    int64_t cap = std::max<int64_t>(
+        prefix, std::min<int64_t>(n, 24 * int64_t(k) * (n / std::max<int64_t>(prefix, 1)) + 4096));
+    cap = std::min<int64_t>(cap, std::max<int64_t>(prefix, (int64_t(4) << 30) / (8 * QB)));
+
+    static thread_local Scratch buf;
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        size_t o = off;
+        off += al256(bytes);
+        return o;
+    };
+    const size_t o_xb = carve(size_t(n_pad) * kp * 2);
+    const size_t o_qb = carve(size_t(q_pad) * kp * 2);
+    const size_t o_xn = carve(size_t(n_pad) * 8);
+    const size_t o_qn = carve(size_t(q_pad) * 8);
+    const size_t o_xx = carve(size_t(n_pad) * 4);
+    const size_t o_qq = carve(size_t(q_pad) * 4);
+    const size_t o_mg = carve(size_t(QB) * 4);
+    const size_t o_th = carve(size_t(QB) * 4);
+    const size_t o_tau = carve(size_t(QB) * 4);
+    const size_t o_cnt = carve(size_t(QB) * 4);
+    const size_t o_cv = carve(size_t(QB) * cap * 4);
+    const size_t o_ci = carve(size_t(QB) * cap * 4);
+    const size_t o_err = carve(16);
+    if (int rc = buf.get(off)) return rc;
+    char *B = static_cast<char *>(buf.p);
+    auto *xb = reinterpret_cast<__nv_bfloat16 *>(B + o_xb);
+    auto *qb = reinterpret_cast<__nv_bfloat16 *>(B + o_qb);
+    auto *xn = reinterpret_cast<double *>(B + o_xn);
+    auto *qn = reinterpret_cast<double *>(B + o_qn);
+    auto *xx = reinterpret_cast<float *>(B + o_xx);
+    auto *qq = reinterpret_cast<float *>(B + o_qq);
+    auto *mg = reinterpret_cast<float *>(B + o_mg);
+    auto *th = reinterpret_cast<float *>(B + o_th);
+    auto *tau = reinterpret_cast<float *>(B + o_tau);
+    auto *cnt = reinterpret_cast<int32_t *>(B + o_cnt);
+    auto *cv = reinterpret_cast<float *>(B + o_cv);
+    auto *ci = reinterpret_cast<int32_t *>(B + o_ci);
+    auto *err = reinterpret_cast<int32_t *>(B + o_err);
+    const T *X = static_cast<const T *>(a->data);
+    const int cos = metric == HNSW_B200_COSINE;
+    int64_t launches = 0;
+
+    prep_rows<T><<<int(std::min<int64_t>(4096, (n_pad + 7) / 8)), 256, 0, s>>>(
+        X, n, dim, n_pad, kp, terms, 0, cos, xb, xn, xx);
+    XT(cudaGetLastError());
+    launches++;
+    double xmax = 1.0;  // largest data norm (margins); one host copy per call
+    if (!cos) {
+        std::vector<double> hn(static_cast<size_t>(n));
+        XT(cudaMemcpyAsync(hn.data(), xn, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
+        XT(cudaStreamSynchronize(s));
+        xmax = 0.0;
+        for (double v : hn) xmax = std::max(xmax, v);
+    }
+    CUtensorMap tmA, tmB;
+    if (int rc = make_map(&tmA, qb, q_pad, kp, BM)) return rc;
+    if (int rc = make_map(&tmB, xb, n_pad, kp, BN)) return rc;
+    const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
+    XT(cudaFuncSetAttribute(knn_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const int wpb = 4;
+    const size_t rsm = size_t(wpb) * (k + 1) * 12;
+    if (rsm > 200 * 1024) return fail(HNSW_B200_EINVAL, "k too large for the rerank kernel");
+    XT(cudaFuncSetAttribute(rerank_topk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(rsm)));
+    XT(cudaMemsetAsync(err, 0, 16, s));
+    std::vector<float> inf(static_cast<size_t>(QB), INFINITY);
+    std::vector<int32_t> hc(static_cast<size_t>(QB));
+    double max_margin = 0.0;
+    int64_t total_cand = 0;
+
+    for (int64_t q0 = 0; q0 < nq_all; q0 += QB) {
+        const int64_t nq = std::min<int64_t>(QB, nq_all - q0);
+        const T *Q = static_cast<const T *>(a->queries) + q0 * dim;
+        prep_rows<T><<<int(std::min<int64_t>(4096, (q_pad + 7) / 8)), 256, 0, s>>>(
+            Q, nq, dim, q_pad, kp, terms, 1, cos, qb, qn, qq);
+        margins_kernel<<<int((nq + 255) / 256), 256, 0, s>>>(qn, int32_t(nq), xmax, kp, terms, metric, mg);
+        XT(cudaGetLastError());
+        launches += 2;
+        auto run_filter = [&](int64_t row_end) -> int {
+            const int tiles = int((row_end + BN - 1) / BN);
+            const int want_splits = std::max(1, (4 * sms + qtiles - 1) / qtiles);
+            const int tps = std::max(1, (tiles + want_splits - 1) / want_splits);
+            const int splits = (tiles + tps - 1) / tps;
+            FilterParams fp;
+            fp.nq = int32_t(nq);
+            fp.row_begin = 0;
+            fp.row_end = int32_t(row_end);
+            fp.kchunks = kp / BK;
+            fp.tiles_per_split = tps;
+            fp.metric = metric;
+            fp.qq = qq;
+            fp.xx = xx;
+            fp.thr = th;
+            fp.cand_val = cv;
+            fp.cand_id = ci;
+            fp.cand_cnt = cnt;
+            fp.cap = int32_t(cap);
+            fp.err = err;
+            XT(cudaMemsetAsync(cnt, 0, size_t(nq) * 4, s));
+            knn_filter_kernel<<<dim3(qtiles, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
+            XT(cudaGetLastError());
+            launches++;
+            return 0;
+        };
+        // Pass one: the prefix rows with no threshold give tau (an upper bound of the k-th).
+        XT(cudaMemcpyAsync(th, inf.data(), size_t(nq) * 4, cudaMemcpyHostToDevice, s));
+        if (int rc = run_filter(prefix)) return rc;
+        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nq), k, mg, th, tau);
+        // Pass two: every row against tau + margin.
+        if (int rc = run_filter(n)) return rc;
+        int32_t herr[4];
+        XT(cudaMemcpyAsync(hc.data(), cnt, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
+        XT(cudaMemcpyAsync(herr, err, 16, cudaMemcpyDeviceToHost, s));
+        XT(cudaStreamSynchronize(s));
+        if (herr[0]) return fail(HNSW_B200_ECUDA, "exact knn: a bounded wait expired in the filter kernel");
+        int32_t worst = 0;
+        for (int64_t i = 0; i < nq; i++) {
+            worst = std::max(worst, hc[size_t(i)]);
+            total_cand += hc[size_t(i)];
+        }
+        if (worst > cap)
+            return fail(HNSW_B200_ERETRY, "exact knn: candidate buffer overflow (" + std::to_string(worst) +
+                                              " > " + std::to_string(cap) + ")");
+        // The k-th smallest candidate is the global k-th approximate distance: final threshold.
+        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nq), k, mg, th, tau);
+        rerank_topk<T><<<int((nq + wpb - 1) / wpb), wpb * 32, rsm, s>>>(
+            X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), th,
+            a->out_ids + q0 * k, a->out_dists + q0 * k);
+        XT(cudaGetLastError());
+        launches += 3;
+        if (a->out_filter_max_error) {
+            std::vector<float> hm(static_cast<size_t>(nq));
+            XT(cudaMemcpyAsync(hm.data(), mg, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
+            XT(cudaStreamSynchronize(s));
+            for (float v : hm) max_margin = std::max(max_margin, double(v));
+        }
+    }
+    if (a->out_filter_max_error) *a->out_filter_max_error = max_margin / 2.0;
+    if (a->out_candidates) *a->out_candidates = total_cand;
+    if (a->out_launches) *a->out_launches = launches;
+    return 0;
+}
+
+}  // namespace hbx
+
+extern "C" int hnsw_b200_exact_knn(const hnsw_b200_exact_args_t *a, void *stream) {
+    using namespace hbx;
+    if (!a || !a->data || !a->queries || !a->out_ids || !a->out_dists)
+        return fail(HNSW_B200_EINVAL, "null argument");
+    if (a->n < 1 || a->n > 0x7ffffff0 || a->dim < 1 || a->k < 1 || a->k > a->n || a->nq < 0)
+        return fail(HNSW_B200_EINVAL, "need n >= 1, dim >= 1, 1 <= k <= n");
+    if (a->metric < 0 || a->metric > 2) return fail(HNSW_B200_EINVAL, "unknown metric");
+    if (a->nq == 0) return 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (a->dtype) {
+        case HNSW_B200_F32: return exact_knn_typed<float>(a, s);
+        case HNSW_B200_U8: return exact_knn_typed<uint8_t>(a, s);
+        default: return fail(HNSW_B200_EINVAL, "unsupported dtype");
+    }
+}

@@ -289,10 +289,11 @@ __device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e
     const bool l2 = P.metric == HNSW_B200_L2;
     const bool vec = (dim & 3) == 0;
     while (umask) {
-        int jj[4];
-        int64_t ee[4];
+        constexpr int NB = 8;  // rows in flight per lane
+        int jj[NB];
+        int64_t ee[NB];
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
+        for (int t = 0; t < NB; t++) {
             if (umask) {
                 jj[t] = __ffs(umask) - 1;
                 umask &= umask - 1;
@@ -301,16 +302,18 @@ __device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e
             }
             ee[t] = __shfl_sync(FULL, e, jj[t] < 0 ? 0 : jj[t]);
         }
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        float acc[NB];
+#pragma unroll
+        for (int t = 0; t < NB; t++) acc[t] = 0.f;
         if (vec) {
             for (int c = lane * 4; c < dim; c += 128) {
                 float4 qv = *reinterpret_cast<const float4 *>(qf + c);
-                float4 xv[4];
+                float4 xv[NB];
 #pragma unroll
-                for (int t = 0; t < 4; t++)
+                for (int t = 0; t < NB; t++)
                     if (jj[t] >= 0) xv[t] = load_row4(P, ee[t], c, U8);
 #pragma unroll
-                for (int t = 0; t < 4; t++) {
+                for (int t = 0; t < NB; t++) {
                     if (jj[t] < 0) continue;
                     if (l2) {
                         float a = xv[t].x - qv.x, b = xv[t].y - qv.y, cc = xv[t].z - qv.z,
@@ -331,7 +334,7 @@ __device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e
             for (int c = lane; c < dim; c += 32) {
                 float qv = qf[c];
 #pragma unroll
-                for (int t = 0; t < 4; t++) {
+                for (int t = 0; t < NB; t++) {
                     if (jj[t] < 0) continue;
                     float x = row_elem(P, ee[t], c, U8);
                     if (l2) {
@@ -344,7 +347,7 @@ __device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e
             }
         }
 #pragma unroll
-        for (int t = 0; t < 4; t++) {
+        for (int t = 0; t < NB; t++) {
             if (jj[t] < 0) continue;  // uniform
             float s = warp_sum(acc[t]);
             double d = l2 ? double(s) : (P.metric == HNSW_B200_IP ? -double(s) : 1.0 - double(s));
@@ -390,14 +393,23 @@ __device__ __forceinline__ uint32_t visit_chunk(const SearchParams &P, Ctx &C, i
 }
 
 __device__ __forceinline__ const int32_t *node_links(const SearchParams &P, int32_t c, int layer,
-                                                     int &cnt) {
+                                                     int &cnt, int &stride) {
     if (layer == 0) {
         cnt = __ldg(P.count0 + c);
+        stride = P.links0_stride;
         return P.links0 + int64_t(c) * P.links0_stride;
     }
     int64_t row = __ldg(P.upper_offset + c) + layer - 1;
     cnt = __ldg(P.count_up + row);
+    stride = P.links_up_stride;
     return P.links_up + row * P.links_up_stride;
+}
+
+// The first chunk of a link row: every lane below the row stride loads its slot in the same round
+// trip as the count (slots past the count are ignored), so the count does not gate the load.
+__device__ __forceinline__ int32_t first_link(const int32_t *nb, int stride, int cnt, int lane) {
+    const int32_t v = lane < stride ? __ldg(nb + lane) : -1;
+    return lane < cnt ? v : -1;
 }
 
 // ------------------------------------------------------------------------- unfiltered layer search
@@ -437,10 +449,11 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
             c = C.ties[tn];  // ties W: expanded after every result (they compare greater)
         }
         C.nhops++;
-        int cnt;
-        const int32_t *nb = node_links(P, c, layer, cnt);
+        int cnt, stride;
+        const int32_t *nb = node_links(P, c, layer, cnt, stride);
         for (int base = 0; base < cnt; base += 32) {
-            const int32_t e = base + lane < cnt ? __ldg(nb + base + lane) : -1;
+            const int32_t e = base == 0 ? first_link(nb, stride, cnt, lane)
+                                        : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
             double dj;
             const uint32_t um = visit_chunk<MODE, U8>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);
@@ -654,7 +667,8 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
         const int cnt = __ldg(P.count0 + c);
         const int32_t *nb = P.links0 + int64_t(c) * P.links0_stride;
         for (int base = 0; base < cnt; base += 32) {
-            const int32_t e = base + lane < cnt ? __ldg(nb + base + lane) : -1;
+            const int32_t e = base == 0 ? first_link(nb, P.links0_stride, cnt, lane)
+                                        : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
             double dj;
             const uint32_t um = visit_chunk<MODE, U8>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);

@@ -89,6 +89,35 @@ typedef struct hnsw_b200_search_args {
     int64_t *out_counters;        /* (nq, 2) int64 distance computations, hops; or NULL */
 } hnsw_b200_search_args_t;
 
+/* Element types of hnsw_b200_exact_knn inputs. */
+#define HNSW_B200_F32 0
+#define HNSW_B200_U8 1
+
+typedef struct hnsw_b200_exact_args {
+    const void *data;              /* (n, dim) rows, dtype below, device memory */
+    const void *queries;           /* (nq, dim) rows, same dtype */
+    int32_t dtype;                 /* HNSW_B200_F32 or HNSW_B200_U8 */
+    int32_t dim;
+    int64_t n;
+    int64_t nq;
+    int32_t k;                     /* 1 <= k <= n */
+    int32_t metric;                /* HNSW_B200_L2 / _IP / _COSINE */
+    int32_t integer_valued;        /* 1: every data and query value is an integer with |v| <= 256
+                                      (exact in BF16: one tensor-core term instead of three) */
+    int32_t reserved;
+    int64_t *out_ids;              /* (nq, k) int64, ascending (distance, id) */
+    double *out_dists;             /* (nq, k) float64 exact distances */
+    double *out_filter_max_error;  /* host: largest error bound of the BF16/FP32 filter, or NULL */
+    int64_t *out_candidates;       /* host: candidates re-scored in float64, or NULL */
+    int64_t *out_launches;         /* host: kernel launches made, or NULL */
+} hnsw_b200_exact_args_t;
+
+/* Exact k nearest neighbours by brute force on the tensor cores (BF16 filter with FP32
+ * accumulation and a derived error margin, then float64 re-rank of the survivors, ties to the
+ * lower id). Replaces oracle.exact_search (src/hnsw_engine/oracle.py:35-126). Synchronises
+ * `stream`. */
+int hnsw_b200_exact_knn(const hnsw_b200_exact_args_t *args, void *stream);
+
 /* Create a search handle over a graph whose arrays live on the current CUDA device. */
 int hnsw_b200_open(const hnsw_b200_graph_t *graph, void **handle);
 
