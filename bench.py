@@ -266,7 +266,7 @@ def main() -> None:
     ids_o = torch.empty((nq, k), dtype=torch.int64, device=dev)
     d_o = torch.empty((nq, k), dtype=torch.float64, device=dev)
     c_o = torch.empty((nq, 2), dtype=torch.int64, device=dev)
-    mode = 1 if g.exact_f32_ok(queries, False) else 0
+    mode = g.choose_mode(queries, False)
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -277,7 +277,7 @@ def main() -> None:
     torch.cuda.synchronize()
     launches_per_step = g.last_launches
     counters = c_o.cpu().numpy()
-    row_bytes = dim * 4
+    row_bytes = dim * (1 if mode == 2 else 4)
     alg_bytes = algorithmic_bytes(counters, arrays, dim, k, row_bytes)
 
     # Device-resident timed region.
@@ -356,7 +356,7 @@ def main() -> None:
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32" if mode == 1 else "f64",
+            "dtype": {2: "u8 (exact int32 dp4a)", 1: "f32 (exact integer)", 0: "f64"}[mode],
             "data": "synthetic",
             "config": {
                 "workload": f"{args.workload}: {arrays['vectors'].shape[0]} x {dim} integer mixture, "

@@ -22,6 +22,7 @@ L2, IP, COSINE = 0, 1, 2
 METRIC_CODES = {"l2": L2, "ip": IP, "cosine": COSINE}
 DIST_F64 = 0
 DIST_EXACT_F32 = 1
+DIST_BYTES = 2
 
 
 class Graph(ctypes.Structure):
@@ -42,6 +43,7 @@ class Graph(ctypes.Structure):
         ("entry_point", ctypes.c_int64),
         ("max_level", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
+        ("vector_bytes", ctypes.c_void_p),
     ]
 
 

@@ -46,12 +46,52 @@ constexpr int32_t EXP_BIT = int32_t(0x80000000u);
 constexpr int32_t ID_MASK = 0x7fffffff;
 constexpr int WPB = 4;  // warps per block
 
+// Minimum resident blocks per SM requested from the compiler (caps registers per thread), per
+// arithmetic mode, and rows in flight per lane in the distance loops. Tuned on B200.
+#ifndef HB_MINB_F64
+#define HB_MINB_F64 6
+#endif
+#ifndef HB_MINB_EXACT
+#define HB_MINB_EXACT 4
+#endif
+#ifndef HB_MINB_BYTES
+#define HB_MINB_BYTES 6
+#endif
+#ifndef HB_NB_EXACT
+#define HB_NB_EXACT 4
+#endif
+#ifndef HB_NB_BYTES
+#define HB_NB_BYTES 16
+#endif
+#ifdef HB_PROFILE
+__device__ unsigned long long hb_prof[8];
+#define HB_PROF_DECL unsigned long long hb_t = clock64();
+#define HB_PROF(i)                                              \
+    do {                                                        \
+        unsigned long long hb_n = clock64();                    \
+        if ((threadIdx.x & 31) == 0) atomicAdd(&hb_prof[i], hb_n - hb_t); \
+        hb_t = hb_n;                                            \
+    } while (0)
+#else
+#define HB_PROF_DECL
+#define HB_PROF(i) \
+    do {           \
+    } while (0)
+#endif
+
+template <int MODE>
+struct MinBlocks {
+    static constexpr int value =
+        MODE == 2 ? HB_MINB_BYTES : (MODE == 1 ? HB_MINB_EXACT : HB_MINB_F64);
+};
+
 enum : int32_t { ST_VISITED = 1, ST_TIES = 2, ST_SPILL = 4 };
-enum : int { MODE_F64 = 0, MODE_EXACT = 1 };
+enum : int { MODE_F64 = 0, MODE_EXACT = 1, MODE_BYTES = 2 };
 
 struct SearchParams {
     const float *vectors;
     const uint8_t *codes;
+    const uint8_t *rows8;  // byte mode: the uint8 rows searched
     const int32_t *links0;
     const int32_t *count0;
     const int64_t *upper_offset;
@@ -78,6 +118,10 @@ struct SearchParams {
     int32_t *n_failed;
     int32_t *queue;
     // scratch (per warp slot)
+    uint32_t *vbits;      // layer-0 visited bitmap, one bit per node, all zero between queries
+    int64_t vbits_stride; // words per slot
+    int32_t *vlist;       // ids marked in the bitmap (to clear them), vlist_cap per slot
+    int32_t vlist_cap;
     int32_t *vis;
     int64_t vis_stride;
     int32_t vis_log2, vis_up_log2;
@@ -91,11 +135,11 @@ struct SearchParams {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// Shared memory of one warp: results, query (f64 and f32), filtered candidates, rerank top-k.
+// Shared memory of one warp: results, query (f64, f32 and bytes), filtered candidates, rerank top-k.
 __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filtered, int s_cap,
                                                   int k_rerank) {
     size_t b = al16(size_t(ef_cap + 1) * 8) + al16(size_t(ef_cap + 1) * 4) + al16(size_t(dim) * 8) +
-               al16(size_t(dim) * 4);
+               al16(size_t(dim) * 4) + al16(size_t(dim));
     if (filtered) b += al16(size_t(s_cap + 1) * 8) + al16(size_t(s_cap + 1) * 4);
     if (k_rerank > 0) b += al16(size_t(k_rerank + 1) * 8) + al16(size_t(k_rerank + 1) * 4);
     return b;
@@ -107,11 +151,15 @@ struct Ctx {
     int32_t *Ri;
     double *qd;
     float *qf;
+    uint32_t *q4;  // query bytes, four per word (byte mode)
     double *Sd;
     int32_t *Si;
     double *Ad;
     int32_t *Ai;
     int32_t *vis;
+    uint32_t *vbits;
+    int32_t *vlist;
+    int32_t vlist_n;  // ids appended to vlist (may exceed the capacity: then clear everything)
     int32_t *ties;
     double *spd;
     int32_t *spi;
@@ -289,7 +337,7 @@ __device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e
     const bool l2 = P.metric == HNSW_B200_L2;
     const bool vec = (dim & 3) == 0;
     while (umask) {
-        constexpr int NB = 8;  // rows in flight per lane
+        constexpr int NB = HB_NB_EXACT;  // rows in flight per lane
         int jj[NB];
         int64_t ee[NB];
 #pragma unroll
@@ -356,11 +404,93 @@ __device__ __forceinline__ void dists_exact_f32(const SearchParams &P, int32_t e
     }
 }
 
+// Byte mode: exact integer distances of uint8 rows to a uint8 query, four dimensions per __dp4a
+// (|x - q| by __vabsdiffu4 for L2) and one warp reduction instruction per row. Lane j (bit j of
+// umask) receives the distance of the neighbour it holds in `e`.
+__device__ __forceinline__ void dists_bytes(const SearchParams &P, int32_t e, uint32_t umask,
+                                            const uint32_t *q4, int lane, double &dj) {
+    const int words = P.dim >> 2;
+    const bool l2 = P.metric == HNSW_B200_L2;
+    const uint32_t *rows = reinterpret_cast<const uint32_t *>(P.rows8);
+    constexpr int NB = HB_NB_BYTES;  // rows in flight per lane
+    if (words <= 32) {
+        // One word of every row per lane: loads of up to NB rows in flight, then one reduction each.
+        const uint32_t q = lane < words ? q4[lane] : 0u;
+        while (umask) {
+            uint32_t x[NB];
+            uint32_t m = umask;
+#pragma unroll
+            for (int t = 0; t < NB; t++) {
+                if (m) {
+                    const int j = __ffs(m) - 1;
+                    m &= m - 1;
+                    const uint32_t ej = uint32_t(__shfl_sync(FULL, e, j));
+                    x[t] = lane < words ? __ldg(rows + size_t(ej) * words + lane) : 0u;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < NB; t++) {
+                if (umask) {  // uniform
+                    const int j = __ffs(umask) - 1;
+                    umask &= umask - 1;
+                    uint32_t a;
+                    if (l2) {
+                        const uint32_t d = __vabsdiffu4(x[t], q);
+                        a = __dp4a(d, d, 0u);
+                    } else {
+                        a = __dp4a(x[t], q, 0u);
+                    }
+                    const uint32_t sum = __reduce_add_sync(FULL, a);
+                    if (lane == j) dj = l2 ? double(sum) : -double(sum);
+                }
+            }
+        }
+        return;
+    }
+    while (umask) {  // wide rows: NB / 2 rows at a time, every lane striding over the words
+        constexpr int NW = NB / 2;
+        int jj[NW];
+        uint32_t acc[NW];
+#pragma unroll
+        for (int t = 0; t < NW; t++) {
+            jj[t] = -1;
+            acc[t] = 0u;
+            if (umask) {
+                jj[t] = __ffs(umask) - 1;
+                umask &= umask - 1;
+            }
+        }
+        for (int w = lane; w < words; w += 32) {
+            const uint32_t q = q4[w];
+#pragma unroll
+            for (int t = 0; t < NW; t++) {
+                if (jj[t] < 0) continue;
+                const uint32_t ej = uint32_t(__shfl_sync(FULL, e, jj[t]));
+                const uint32_t x = __ldg(rows + size_t(ej) * words + w);
+                if (l2) {
+                    const uint32_t d = __vabsdiffu4(x, q);
+                    acc[t] = __dp4a(d, d, acc[t]);
+                } else {
+                    acc[t] = __dp4a(x, q, acc[t]);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < NW; t++) {
+            if (jj[t] < 0) continue;  // uniform
+            const uint32_t sum = __reduce_add_sync(FULL, acc[t]);
+            if (lane == jj[t]) dj = l2 ? double(sum) : -double(sum);
+        }
+    }
+}
+
 // Distance of one node held uniformly by the warp.
 template <int MODE, bool U8>
 __device__ __forceinline__ double dist_one(const SearchParams &P, Ctx &C, int32_t e) {
     double d = 0.0;
-    if (MODE == MODE_EXACT) {
+    if (MODE == MODE_BYTES) {
+        dists_bytes(P, e, 1u, C.q4, C.lane, d);
+    } else if (MODE == MODE_EXACT) {
         dists_exact_f32<U8>(P, e, 1u, C.qf, C.lane, d);
     } else if (C.lane == 0) {
         d = dist_seq_f64<U8>(P, e, C.qd);
@@ -368,28 +498,74 @@ __device__ __forceinline__ double dist_one(const SearchParams &P, Ctx &C, int32_
     return __shfl_sync(FULL, d, 0);
 }
 
-// Mark one chunk of up to 32 neighbours visited (first occurrence wins) and score the new ones.
-// Returns the mask of lanes holding a newly visited neighbour; its distance is in dj.
-template <int MODE, bool U8>
-__device__ __forceinline__ uint32_t visit_chunk(const SearchParams &P, Ctx &C, int32_t e, int log2,
-                                                int &vis_count, double &dj) {
+// Mark one chunk of up to 32 neighbours visited (first occurrence in stored order wins). Returns
+// the mask of lanes holding a newly visited neighbour.
+// log2 > 0: the open-addressing hash of the upper layers; log2 == 0: the layer-0 bitmap (one
+// atomicOr per neighbour, no probing), whose marked ids are listed so they can be cleared.
+__device__ __forceinline__ uint32_t mark_chunk(const SearchParams &P, Ctx &C, int32_t e, int log2,
+                                               int &vis_count) {
     const bool has = e >= 0;
     const uint32_t hmask = __ballot_sync(FULL, has);
     int ins = 0;
     if (has) {
         uint32_t same = __match_any_sync(hmask, e);
-        if (__ffs(same) - 1 == C.lane) ins = vis_insert(C.vis, log2, e);
+        if (__ffs(same) - 1 == C.lane) {
+            if (log2 > 0) {
+                ins = vis_insert(C.vis, log2, e);
+            } else {
+                const uint32_t bit = 1u << (e & 31);
+                ins = (atomicOr(C.vbits + (e >> 5), bit) & bit) ? 0 : 1;
+            }
+        }
     }
     const uint32_t umask = __ballot_sync(FULL, ins == 1);
-    if (__any_sync(FULL, ins < 0)) C.status |= ST_VISITED;
+    if (log2 > 0) {
+        if (__any_sync(FULL, ins < 0)) C.status |= ST_VISITED;
+    } else if (umask) {
+        const int o = C.vlist_n + __popc(umask & ((1u << C.lane) - 1u));
+        if (ins == 1 && o < P.vlist_cap) C.vlist[o] = e;
+        C.vlist_n += __popc(umask);
+    }
     vis_count += __popc(umask);
+    return umask;
+}
+
+// Layer-0 bitmap: mark the entry node.
+__device__ __forceinline__ void bitmap_begin(const SearchParams &P, Ctx &C, int32_t e0) {
+    C.vlist_n = 1;
+    if (C.lane == 0) {
+        atomicOr(C.vbits + (e0 >> 5), 1u << (e0 & 31));
+        if (P.vlist_cap > 0) C.vlist[0] = e0;
+    }
+    __syncwarp();
+}
+
+// Layer-0 bitmap: return every bit this query set to zero (listed words, or the whole bitmap when
+// the list overflowed), so the next query starts from an empty set.
+__device__ __forceinline__ void bitmap_clear(const SearchParams &P, Ctx &C) {
+    __syncwarp();
+    if (C.vlist_n <= P.vlist_cap) {
+        for (int i = C.lane; i < C.vlist_n; i += 32) C.vbits[C.vlist[i] >> 5] = 0u;
+    } else {
+        int4 *w4 = reinterpret_cast<int4 *>(C.vbits);
+        const int64_t n4 = P.vbits_stride >> 2;
+        for (int64_t i = C.lane; i < n4; i += 32) w4[i] = make_int4(0, 0, 0, 0);
+    }
+    __syncwarp();
+}
+
+// Distances of the newly visited neighbours: lane j (bit j of umask) receives its distance in dj.
+template <int MODE, bool U8>
+__device__ __forceinline__ void score_chunk(const SearchParams &P, Ctx &C, int32_t e, uint32_t umask,
+                                            double &dj) {
     dj = 0.0;
-    if (MODE == MODE_EXACT) {
+    if (MODE == MODE_BYTES) {
+        dists_bytes(P, e, umask, C.q4, C.lane, dj);
+    } else if (MODE == MODE_EXACT) {
         dists_exact_f32<U8>(P, e, umask, C.qf, C.lane, dj);
-    } else if (ins == 1) {
+    } else if ((umask >> C.lane) & 1u) {
         dj = dist_seq_f64<U8>(P, e, C.qd);
     }
-    return umask;
 }
 
 __device__ __forceinline__ const int32_t *node_links(const SearchParams &P, int32_t c, int layer,
@@ -418,15 +594,22 @@ __device__ __forceinline__ int32_t first_link(const int32_t *nb, int stride, int
 template <int MODE, bool U8>
 __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, int log2, int &r) {
     const int lane = C.lane;
-    vis_clear(C.vis, log2, lane);
-    if (lane == 0) vis_insert(C.vis, log2, C.Ri[0] & ID_MASK);
-    __syncwarp();
+    if (layer > 0) {
+        vis_clear(C.vis, log2, lane);
+        if (lane == 0) vis_insert(C.vis, log2, C.Ri[0] & ID_MASK);
+        __syncwarp();
+    } else {
+        log2 = 0;  // bitmap
+        bitmap_begin(P, C, C.Ri[0] & ID_MASK);
+    }
     int vis_count = 1;
-    const int vis_lim = ((1 << log2) >> 2) * 3;
+    const int vis_lim = log2 > 0 ? ((1 << log2) >> 2) * 3 : 0x7fffffff;
     double W = C.Rd[r - 1];
     int scan = 0;  // every result before `scan` is expanded
     int tn = 0;    // tie stack depth
+    HB_PROF_DECL
     for (;;) {
+        HB_PROF(0);
         int32_t c = -1;
         while (scan < r) {
             const int i = scan + lane;
@@ -449,13 +632,25 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
             c = C.ties[tn];  // ties W: expanded after every result (they compare greater)
         }
         C.nhops++;
+        HB_PROF(1);
         int cnt, stride;
         const int32_t *nb = node_links(P, c, layer, cnt, stride);
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? first_link(nb, stride, cnt, lane)
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
+#ifdef HB_PROFILE
+            __syncwarp();
+            if (__shfl_sync(FULL, e, 0) == -2) C.status |= 64;  // consume the load before timing
+#endif
+            HB_PROF(2);
+            const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
+            HB_PROF(3);
             double dj;
-            const uint32_t um = visit_chunk<MODE, U8>(P, C, e, log2, vis_count, dj);
+            score_chunk<MODE, U8>(P, C, e, um, dj);
+#ifdef HB_PROFILE
+            if (__shfl_sync(FULL, dj, 0) == -12345.0) C.status |= 64;  // consume before timing
+#endif
+            HB_PROF(5);
             C.ndist += __popc(um);
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
@@ -493,6 +688,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
                 W = C.Rd[r - 1];
                 if (r == ef) am &= __ballot_sync(FULL, dj < W);
             }
+            HB_PROF(4);
         }
         if (vis_count > vis_lim) C.status |= ST_VISITED;
         if (C.status) break;
@@ -637,9 +833,9 @@ template <int MODE, bool U8>
 __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2, double d0,
                                 int32_t e0, int &r) {
     const int lane = C.lane;
-    vis_clear(C.vis, log2, lane);
+    log2 = 0;  // bitmap
+    bitmap_begin(P, C, e0);
     if (lane == 0) {
-        vis_insert(C.vis, log2, e0);
         C.Sd[0] = d0;
         C.Si[0] = e0;
         if (is_allowed(P.allowed, e0)) {
@@ -651,7 +847,7 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
     r = is_allowed(P.allowed, e0) ? 1 : 0;
     Cands K{1, 0, INFINITY, 0x7fffffff};
     int vis_count = 1;
-    const int vis_lim = ((1 << log2) >> 2) * 3;
+    const int vis_lim = 0x7fffffff;
     double W = r > 0 ? C.Rd[r - 1] : INFINITY;
     for (;;) {
         if (K.s == 0) {
@@ -669,8 +865,9 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? first_link(nb, P.links0_stride, cnt, lane)
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
+            const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
             double dj;
-            const uint32_t um = visit_chunk<MODE, U8>(P, C, e, log2, vis_count, dj);
+            score_chunk<MODE, U8>(P, C, e, um, dj);
             C.ndist += __popc(um);
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
@@ -735,7 +932,7 @@ __device__ int rerank_epilogue(const SearchParams &P, Ctx &C, int m) {
 
 // --------------------------------------------------------------------------------------- kernel
 template <int MODE, bool U8, bool FILT>
-__global__ void __launch_bounds__(WPB * 32) search_kernel(const SearchParams P) {
+__global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kernel(const SearchParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -752,6 +949,8 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(const SearchParams P) 
     p += al16(size_t(P.dim) * 8);
     C.qf = reinterpret_cast<float *>(p);
     p += al16(size_t(P.dim) * 4);
+    C.q4 = reinterpret_cast<uint32_t *>(p);
+    p += al16(size_t(P.dim));
     C.Sd = nullptr;
     C.Si = nullptr;
     if (FILT) {
@@ -765,6 +964,9 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(const SearchParams P) 
     C.Ai = reinterpret_cast<int32_t *>(p);
     const int64_t slot = int64_t(blockIdx.x) * WPB + warp;
     C.vis = P.vis + slot * P.vis_stride;
+    C.vbits = P.vbits + slot * P.vbits_stride;
+    C.vlist = P.vlist + slot * P.vlist_cap;
+    C.vlist_n = 0;
     C.ties = P.ties + slot * P.tie_cap;
     C.spd = FILT ? P.spill_d + slot * P.spill_cap : nullptr;
     C.spi = FILT ? P.spill_i + slot * P.spill_cap : nullptr;
@@ -776,17 +978,20 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(const SearchParams P) 
         if (w >= P.n_work) break;
         const int q = P.qlist ? P.qlist[w] : w;
         const int dim = P.dim;
+        uint8_t *qb = reinterpret_cast<uint8_t *>(C.q4);
         if (P.queries_f64) {
             const double *src = static_cast<const double *>(P.queries) + int64_t(q) * dim;
             for (int i = lane; i < dim; i += 32) {
                 C.qd[i] = src[i];
                 C.qf[i] = float(src[i]);
+                if (MODE == MODE_BYTES) qb[i] = uint8_t(src[i]);
             }
         } else {
             const float *src = static_cast<const float *>(P.queries) + int64_t(q) * dim;
             for (int i = lane; i < dim; i += 32) {
                 C.qd[i] = double(src[i]);
                 C.qf[i] = src[i];
+                if (MODE == MODE_BYTES) qb[i] = uint8_t(src[i]);
             }
         }
         __syncwarp();
@@ -823,6 +1028,7 @@ __global__ void __launch_bounds__(WPB * 32) search_kernel(const SearchParams P) 
                 r = 1;
                 layer_search<MODE, U8>(P, C, 0, ef0, P.vis_log2, r);
             }
+            bitmap_clear(P, C);
         }
         if (C.status) {
             if (lane == 0) {
@@ -888,7 +1094,8 @@ int fail(int code, const std::string &msg) {
 struct Buffer {
     void *ptr = nullptr;
     size_t bytes = 0;
-    int ensure(size_t want) {
+    // Grow to at least `want` bytes; a new allocation is zero-filled when `zero` (on `s`).
+    int ensure(size_t want, bool zero = false, cudaStream_t s = nullptr) {
         if (want <= bytes) return 0;
         if (ptr) cudaFree(ptr);
         ptr = nullptr;
@@ -899,6 +1106,8 @@ struct Buffer {
             return fail(HNSW_B200_ENOMEM, "cudaMalloc of " + std::to_string(b) + " bytes failed");
         }
         bytes = b;
+        if (zero && cudaMemsetAsync(ptr, 0, b, s) != cudaSuccess)
+            return fail(HNSW_B200_ECUDA, "cudaMemsetAsync of new scratch failed");
         return 0;
     }
     void release() {
@@ -915,7 +1124,8 @@ struct Handle {
     Buffer counters;  // queue, n_failed, n_list
     Buffer status;
     Buffer qlist[2];  // retry work lists (ping-pong)
-    Buffer vis, ties, spill_d, spill_i;
+    Buffer vis, ties, spill_d, spill_i, vbits, vlist;
+    bool bits_dirty = false;  // a launch failed mid-flight: bitmaps must be re-zeroed
     int32_t *host_pinned = nullptr;  // 4 ints
     long long launches = 0;
     std::mutex mu;
@@ -941,6 +1151,7 @@ int launch_mode(Handle &h, const SearchParams &P, bool filt, size_t smem_block, 
 
 int dispatch(Handle &h, const SearchParams &P, int mode, bool u8, bool filt, size_t smem_block,
              int blocks, cudaStream_t s) {
+    if (mode == MODE_BYTES) return launch_mode<MODE_BYTES, true>(h, P, filt, smem_block, blocks, s);
     if (mode == MODE_EXACT)
         return u8 ? launch_mode<MODE_EXACT, true>(h, P, filt, smem_block, blocks, s)
                   : launch_mode<MODE_EXACT, false>(h, P, filt, smem_block, blocks, s);
@@ -959,6 +1170,9 @@ int occupancy_of(size_t smem_block, int *blocks_per_sm) {
 }
 
 int occupancy(int mode, bool u8, bool filt, size_t smem_block, int *bps) {
+    if (mode == MODE_BYTES)
+        return filt ? occupancy_of<2, true, true>(smem_block, bps)
+                    : occupancy_of<2, true, false>(smem_block, bps);
     if (mode == MODE_EXACT) {
         if (u8) return filt ? occupancy_of<1, true, true>(smem_block, bps)
                             : occupancy_of<1, true, false>(smem_block, bps);
@@ -982,6 +1196,17 @@ int ilog2_ceil(int64_t x) {
 using namespace hb;
 
 extern "C" {
+
+#ifdef HB_PROFILE
+int hnsw_b200_prof_read(unsigned long long *out, int reset) {
+    cudaMemcpyFromSymbol(out, hb::hb_prof, sizeof(unsigned long long) * 8);
+    if (reset) {
+        unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        cudaMemcpyToSymbol(hb::hb_prof, z, sizeof(z));
+    }
+    return 0;
+}
+#endif
 
 const char *hnsw_b200_last_error(void) { return hb::g_err.c_str(); }
 
@@ -1020,6 +1245,8 @@ void hnsw_b200_close(void *handle) {
     h->qlist[0].release();
     h->qlist[1].release();
     h->vis.release();
+    h->vbits.release();
+    h->vlist.release();
     h->ties.release();
     h->spill_d.release();
     h->spill_i.release();
@@ -1044,13 +1271,18 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     if (!a->queries || !a->ef || !a->out_ids || !a->out_dists)
         return fail(HNSW_B200_EINVAL, "queries, ef and outputs must be device pointers");
     if (a->use_codes && !g.codes) return fail(HNSW_B200_EINVAL, "graph has no codes");
-    if (a->dist_mode != HNSW_B200_DIST_F64 && a->dist_mode != HNSW_B200_DIST_EXACT_F32)
+    if (a->dist_mode < HNSW_B200_DIST_F64 || a->dist_mode > HNSW_B200_DIST_BYTES)
         return fail(HNSW_B200_EINVAL, "unknown dist_mode");
-    if (a->dist_mode == HNSW_B200_DIST_EXACT_F32 && g.metric == HNSW_B200_COSINE)
-        return fail(HNSW_B200_EINVAL, "exact float32 mode needs integer data (not cosine)");
+    if (a->dist_mode != HNSW_B200_DIST_F64 && g.metric == HNSW_B200_COSINE)
+        return fail(HNSW_B200_EINVAL, "exact integer modes need integer data (not cosine)");
+    const uint8_t *rows8 = a->use_codes ? g.codes : g.vector_bytes;
+    if (a->dist_mode == HNSW_B200_DIST_BYTES && (!rows8 || (g.dim & 3)))
+        return fail(HNSW_B200_EINVAL, "byte mode needs uint8 rows and dim a multiple of 4");
     const bool filt = a->allowed != nullptr;
     const bool u8 = a->use_codes != 0;
-    const int mode = a->dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64;
+    const int mode = a->dist_mode == HNSW_B200_DIST_BYTES
+                         ? MODE_BYTES
+                         : (a->dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64);
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
     const int s_cap = 256;
@@ -1071,6 +1303,8 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     int vis_log2 = std::max(8, ilog2_ceil(int64_t(2.0 * est)));
     int vis_up_log2 = 10;
     int tie_cap = ef_cap + 64;
+    const int64_t vbits_stride = ((g.n + 31) / 32 + 3) / 4 * 4;
+    const int vlist_cap = int(std::min<int64_t>(65536, std::max<int64_t>(256, g.n / 256)));
     int spill_cap = filt ? int(std::min(double(g.n) + 64.0, est)) : 0;
 
     if (int rc = h.counters.ensure(4 * sizeof(int32_t))) return rc;
@@ -1083,6 +1317,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     std::memset(&P, 0, sizeof(P));
     P.vectors = g.vectors;
     P.codes = g.codes;
+    P.rows8 = rows8;
     P.links0 = g.links0;
     P.count0 = g.count0;
     P.upper_offset = g.upper_offset;
@@ -1118,11 +1353,21 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         const int64_t slots = int64_t(blocks) * WPB;
         const int64_t vis_stride = int64_t(1) << std::max(vis_log2, vis_up_log2);
         if (int rc = h.vis.ensure(size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
+        if (h.bits_dirty && h.vbits.ptr) {
+            CUDA_TRY(cudaMemsetAsync(h.vbits.ptr, 0, h.vbits.bytes, s));
+            h.bits_dirty = false;
+        }
+        if (int rc = h.vbits.ensure(size_t(slots * vbits_stride) * sizeof(uint32_t), true, s)) return rc;
+        if (int rc = h.vlist.ensure(size_t(slots) * vlist_cap * sizeof(int32_t))) return rc;
         if (int rc = h.ties.ensure(size_t(slots) * tie_cap * sizeof(int32_t))) return rc;
         if (filt) {
             if (int rc = h.spill_d.ensure(size_t(slots) * spill_cap * sizeof(double))) return rc;
             if (int rc = h.spill_i.ensure(size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
         }
+        P.vbits = static_cast<uint32_t *>(h.vbits.ptr);
+        P.vbits_stride = vbits_stride;
+        P.vlist = static_cast<int32_t *>(h.vlist.ptr);
+        P.vlist_cap = vlist_cap;
         P.vis = static_cast<int32_t *>(h.vis.ptr);
         P.vis_stride = vis_stride;
         P.vis_log2 = vis_log2;
@@ -1135,9 +1380,16 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         P.qlist = qlist;
         P.n_work = n_work;
         CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(int32_t), s));
-        if (int rc = dispatch(h, P, mode, u8, filt, smem_block, blocks, s)) return rc;
+        if (int rc = dispatch(h, P, mode, u8, filt, smem_block, blocks, s)) {
+            h.bits_dirty = true;
+            return rc;
+        }
         CUDA_TRY(cudaMemcpyAsync(h.host_pinned, ctr, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            h.bits_dirty = true;
+            return fail(HNSW_B200_ECUDA, std::string("search kernel failed: ") +
+                                             cudaGetErrorString(cudaGetLastError()));
+        }
         const int32_t failed = h.host_pinned[1];
         if (failed == 0) return 0;
         // Re-run the overflowed queries with four times the scratch of every kind.

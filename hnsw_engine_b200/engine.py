@@ -90,10 +90,17 @@ class DeviceGraph:
             self.count_up = to_device(count_up, torch.int32, self.device)
         self.links0_stride = int(arrays["links0"].shape[1])
         self.codes: torch.Tensor | None = None
-        # Host facts for choosing the exact float32 kernel.
+        # Host facts for choosing the exact integer kernels.
         self._integer = bool(np.array_equal(host_vectors, np.rint(host_vectors)))
         self._lo = host_vectors.min(axis=0).astype(np.float64) if self.n else np.zeros(self.dim)
         self._hi = host_vectors.max(axis=0).astype(np.float64) if self.n else np.zeros(self.dim)
+        # Integer vectors in [0, 255] are the same values as bytes: keep a uint8 copy so the byte
+        # kernel (exact integer dot products) can search them with a quarter of the traffic.
+        self.vector_bytes: torch.Tensor | None = None
+        if (self._integer and self.n and self.dim % 4 == 0 and self._lo.min() >= 0
+                and self._hi.max() <= 255):
+            with torch.cuda.device(self.device):
+                self.vector_bytes = to_device(host_vectors.astype(np.uint8), torch.uint8, self.device)
         self._handle = ctypes.c_void_p()
         self._open()
 
@@ -115,6 +122,7 @@ class DeviceGraph:
             entry_point=self.entry_point,
             max_level=self.max_level,
             reserved=0,
+            vector_bytes=_dev_ptr(self.vector_bytes),
         )
 
     def _open(self) -> None:
@@ -149,6 +157,15 @@ class DeviceGraph:
         return int(self.lib.hnsw_b200_last_launches(self._handle))
 
     # ------------------------------------------------------------------ arithmetic selection
+    def choose_mode(self, queries: NDArray[Any], codes: bool) -> int:
+        """Fastest exact arithmetic for this batch: bytes, exact float32, or float64 sequential."""
+        if self.metric != "cosine" and self.dim % 4 == 0:
+            rows_ok = codes or self.vector_bytes is not None
+            q = np.asarray(queries)
+            if rows_ok and q.size and np.array_equal(q, np.rint(q)) and q.min() >= 0 and q.max() <= 255:
+                return _lib.DIST_BYTES
+        return _lib.DIST_EXACT_F32 if self.exact_f32_ok(queries, codes) else _lib.DIST_F64
+
     def exact_f32_ok(self, queries: NDArray[Any], codes: bool, step_lo_hi=None) -> bool:
         """Whether float32 arithmetic is exact for this batch (integer data, partial sums < 2**24)."""
         if self.metric == "cosine":
@@ -200,7 +217,7 @@ class DeviceGraph:
         q_f64 = use_codes
         if dist_mode is None:
             host_q = queries.detach().cpu().numpy() if isinstance(queries, torch.Tensor) else queries
-            dist_mode = _lib.DIST_EXACT_F32 if self.exact_f32_ok(host_q, use_codes) else _lib.DIST_F64
+            dist_mode = self.choose_mode(host_q, use_codes)
         with torch.cuda.device(dev):
             q = to_device(queries, torch.float64 if q_f64 else torch.float32, dev)
             if isinstance(ef, torch.Tensor):

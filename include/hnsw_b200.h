@@ -60,6 +60,8 @@ typedef struct hnsw_b200_graph {
     int64_t entry_point;
     int32_t max_level;
     int32_t reserved;
+    const uint8_t *vector_bytes; /* (n, dim) uint8 copy of integer-valued vectors in [0, 255] (the
+                                    same values, one byte each), or NULL; enables the byte mode */
 } hnsw_b200_graph_t;
 
 /* Distance arithmetic of one search call. */
@@ -68,6 +70,10 @@ typedef struct hnsw_b200_graph {
 #define HNSW_B200_DIST_EXACT_F32 1 /* float32 with warp-parallel sums; the caller asserts that data
                                      and queries are integer-valued with every partial sum below
                                      2^24, so the result is the same exact integer */
+#define HNSW_B200_DIST_BYTES 2     /* integer dot products of uint8 rows (graph->codes with use_codes,
+                                     else graph->vector_bytes) and uint8 queries (__dp4a): exact; the
+                                     caller asserts the queries are integers in [0, 255] and dim is a
+                                     multiple of 4 */
 
 typedef struct hnsw_b200_search_args {
     const void *queries;          /* (nq, dim): float32, or float64 if queries_f64 */

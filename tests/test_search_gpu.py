@@ -38,9 +38,9 @@ def test_search_matches_reference_bit_for_bit(name: str) -> None:
         np.testing.assert_array_equal([st.distance_computations, st.hops], case[f"ctr_m{mi}_ef{ef}"])
 
 
-@pytest.mark.parametrize("mode", [0, 1])
-def test_both_arithmetic_modes_agree_on_integer_data(mode: int) -> None:
-    """The float64-sequential kernel and the exact float32 kernel give identical results."""
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_every_arithmetic_mode_agrees_on_integer_data(mode: int) -> None:
+    """Float64-sequential, exact float32 and byte (dp4a) kernels give identical results."""
     case = load_golden("search_mix10k")
     arrays, ep, ml = case_arrays(case, "mix10k")
     index = _index(arrays, ep, ml, "l2", 16)
