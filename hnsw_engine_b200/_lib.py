@@ -64,6 +64,13 @@ class SearchArgs(ctypes.Structure):
         ("out_ids", ctypes.c_void_p),
         ("out_dists", ctypes.c_void_p),
         ("out_counters", ctypes.c_void_p),
+        ("stop_mlp", ctypes.c_void_p),
+        ("stop_threshold", ctypes.c_float),
+        ("trace_cap", ctypes.c_int32),
+        ("trace_feat", ctypes.c_void_p),
+        ("trace_dk", ctypes.c_void_p),
+        ("trace_count", ctypes.c_void_p),
+        ("trace_hops", ctypes.c_void_p),
     ]
 
 
@@ -93,6 +100,19 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "hnsw_b200_close": (None, [ctypes.c_void_p]),
     "hnsw_b200_search": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchArgs), ctypes.c_void_p]),
     "hnsw_b200_exact_knn": (ctypes.c_int, [ctypes.POINTER(ExactArgs), ctypes.c_void_p]),
+    "hnsw_b200_mlp_param_count": (ctypes.c_int64, []),
+    "hnsw_b200_mlp_packed_bytes": (ctypes.c_int64, []),
+    "hnsw_b200_mlp_scratch_bytes": (ctypes.c_int64, [ctypes.c_int32]),
+    "hnsw_b200_mlp_train_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_int64, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "hnsw_b200_mlp_gradients": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 ctypes.c_void_p]),
+    "hnsw_b200_mlp_predict": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                               ctypes.c_void_p, ctypes.c_void_p]),
+    "hnsw_b200_mlp_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
     "hnsw_b200_last_error": (ctypes.c_char_p, []),
     "hnsw_b200_version": (ctypes.c_char_p, []),

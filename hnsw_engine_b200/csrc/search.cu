@@ -26,6 +26,7 @@
 //    resident), cleared per layer, as the reference's epoch-stamped array is per layer.
 // Any capacity overflow sets a per-query status bit; the host re-runs those queries with larger
 // scratch, so results are always exact. Nothing traps and every loop is bounded.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -131,7 +132,28 @@ struct SearchParams {
     int32_t *spill_i;
     int32_t spill_cap;
     int32_t s_cap;
+    // learned early termination (layer 0, unfiltered): features every STOP_EVERY expansions
+    const void *stop_mlp;   // packed network (see mlp_smem_bytes), or NULL
+    float stop_threshold;   // stop once the predicted log1p(remaining checkpoints) falls below it
+    float *trace_feat;      // (n_queries, trace_cap, STOP_FEATURES) or NULL
+    double *trace_dk;       // (n_queries, trace_cap): k-th result distance at each checkpoint
+    int32_t *trace_count;   // (n_queries,) checkpoints recorded
+    int32_t *trace_hops;    // (n_queries,) layer-0 expansions of the whole search
+    int32_t trace_cap;
 };
+
+constexpr int STOP_EVERY = 16;
+constexpr int STOP_FEATURES = 12;
+constexpr int STOP_HIDDEN = 64;
+// Packed network in device memory: bf16 W1^T (12 x 64), bf16 W2^T (64 x 64), bf16 W3 (64), then
+// float32 b1 (64), b2 (64), b3 (1), feature mean (12), feature 1/std (12). Transposed so lane j
+// reads column j without bank conflicts; features are standardised in the kernel.
+constexpr int MLP_W1 = STOP_FEATURES * STOP_HIDDEN;
+constexpr int MLP_W2 = STOP_HIDDEN * STOP_HIDDEN;
+constexpr int MLP_W3 = STOP_HIDDEN;
+constexpr int MLP_BF16 = MLP_W1 + MLP_W2 + MLP_W3;           // 4928 bf16 values
+constexpr int MLP_F32 = STOP_HIDDEN + STOP_HIDDEN + 1 + 2 * STOP_FEATURES;  // 153 floats
+constexpr size_t MLP_BYTES = size_t(MLP_BF16) * 2 + size_t(MLP_F32) * 4;
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -165,6 +187,10 @@ struct Ctx {
     int32_t *spi;
     long long ndist, nhops;  // uniform across the warp
     int32_t status;          // uniform across the warp
+    int32_t q;               // query row
+    float qfeat;             // log1p(|q|^2), a stop feature
+    const __nv_bfloat16 *mlp_w;  // block shared memory copy of the network (or NULL)
+    const float *mlp_b;
 };
 
 __device__ __forceinline__ bool pair_lt(double da, int32_t ia, double db, int32_t ib) {
@@ -588,6 +614,97 @@ __device__ __forceinline__ int32_t first_link(const int32_t *nb, int stride, int
     return lane < cnt ? v : -1;
 }
 
+// ------------------------------------------------------------------------ learned early termination
+// Warp matvec of the 12 -> 64 -> 64 -> 1 ReLU network: BF16 weights, FP32 accumulation. Every lane
+// holds the same (uniform) features; lane j computes hidden units j and j + 32.
+__device__ __forceinline__ float mlp_eval(const Ctx &C, const float (&raw)[STOP_FEATURES]) {
+    const int lane = C.lane;
+    const __nv_bfloat16 *w1t = C.mlp_w;             // [i][j]
+    const __nv_bfloat16 *w2t = w1t + MLP_W1;        // [i][j]
+    const __nv_bfloat16 *w3 = w2t + MLP_W2;
+    const float *b1 = C.mlp_b, *b2 = b1 + STOP_HIDDEN, *b3 = b2 + STOP_HIDDEN;
+    const float *mu = b3 + 1, *inv_sd = mu + STOP_FEATURES;
+    float f[STOP_FEATURES];
+#pragma unroll
+    for (int i = 0; i < STOP_FEATURES; i++) f[i] = (raw[i] - mu[i]) * inv_sd[i];
+    float ha = b1[lane], hb = b1[lane + 32];
+#pragma unroll
+    for (int i = 0; i < STOP_FEATURES; i++) {
+        ha = fmaf(__bfloat162float(w1t[i * STOP_HIDDEN + lane]), f[i], ha);
+        hb = fmaf(__bfloat162float(w1t[i * STOP_HIDDEN + lane + 32]), f[i], hb);
+    }
+    ha = fmaxf(ha, 0.f);
+    hb = fmaxf(hb, 0.f);
+    float ga = b2[lane], gb = b2[lane + 32];
+#pragma unroll 8
+    for (int i = 0; i < 32; i++) {
+        const float x = __shfl_sync(FULL, ha, i);
+        const float y = __shfl_sync(FULL, hb, i);
+        ga = fmaf(__bfloat162float(w2t[i * STOP_HIDDEN + lane]), x, ga);
+        gb = fmaf(__bfloat162float(w2t[i * STOP_HIDDEN + lane + 32]), x, gb);
+        ga = fmaf(__bfloat162float(w2t[(i + 32) * STOP_HIDDEN + lane]), y, ga);
+        gb = fmaf(__bfloat162float(w2t[(i + 32) * STOP_HIDDEN + lane + 32]), y, gb);
+    }
+    ga = fmaxf(ga, 0.f);
+    gb = fmaxf(gb, 0.f);
+    float o = __bfloat162float(w3[lane]) * ga + __bfloat162float(w3[lane + 32]) * gb;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) o += __shfl_xor_sync(FULL, o, off);
+    return o + b3[0];
+}
+
+// Search-progress state of layer 0 for the stop features.
+struct StopState {
+    int hops0;        // layer-0 expansions
+    int churn;        // admissions into the first k results since the last checkpoint
+    int cp;           // checkpoints taken
+    float dk_prev, dk_prev2, d_entry;
+};
+
+// At a checkpoint: features, optional trace row, optional network decision (true = stop).
+__device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, StopState &S, int r,
+                                                int scan, double W) {
+    const int lane = C.lane;
+    const int kk = min(r, P.k);
+    const float dk = log1pf(float(C.Rd[kk - 1]));
+    const float d1 = log1pf(float(C.Rd[0]));
+    // Frontier: distance of the next candidate the search would expand (the worst if none).
+    double dn = W;
+    for (int b = scan; b < r; b += 32) {
+        const int i = b + lane;
+        const uint32_t m = __ballot_sync(FULL, i < r && !(C.Ri[i] & EXP_BIT));
+        if (m) {
+            dn = C.Rd[b + __ffs(m) - 1];
+            break;
+        }
+    }
+    float f[STOP_FEATURES];
+    f[0] = d1;
+    f[1] = dk;
+    f[2] = (S.cp > 0 ? S.dk_prev : S.d_entry) - dk;
+    f[3] = (S.cp > 1 ? S.dk_prev2 : S.d_entry) - dk;
+    f[4] = float(S.hops0) * (1.f / 64.f);
+    f[5] = float(C.ndist) * (1.f / 1024.f);
+    f[6] = S.d_entry;
+    f[7] = C.qfeat;
+    f[8] = dk - S.d_entry;
+    f[9] = d1 - dk;
+    f[10] = float(S.churn) * (1.f / STOP_EVERY);
+    f[11] = log1pf(float(dn)) - dk;
+    if (P.trace_feat && S.cp < P.trace_cap && lane == 0) {
+        float *row = P.trace_feat + (int64_t(C.q) * P.trace_cap + S.cp) * STOP_FEATURES;
+#pragma unroll
+        for (int i = 0; i < STOP_FEATURES; i++) row[i] = f[i];
+        P.trace_dk[int64_t(C.q) * P.trace_cap + S.cp] = C.Rd[kk - 1];
+    }
+    S.cp++;
+    S.dk_prev2 = S.dk_prev;
+    S.dk_prev = dk;
+    S.churn = 0;
+    if (C.mlp_w && r >= P.k) return mlp_eval(C, f) < P.stop_threshold;
+    return false;
+}
+
 // ------------------------------------------------------------------------- unfiltered layer search
 // Algorithm 2 with exact reference semantics. On entry R[0] holds the single entry node
 // (unexpanded) and r == 1; on exit R[0..r) is the sorted result list.
@@ -607,6 +724,8 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
     double W = C.Rd[r - 1];
     int scan = 0;  // every result before `scan` is expanded
     int tn = 0;    // tie stack depth
+    const bool track = layer == 0 && (P.trace_feat != nullptr || C.mlp_w != nullptr);
+    StopState S{0, 0, 0, 0.f, 0.f, log1pf(float(C.Rd[0]))};
     HB_PROF_DECL
     for (;;) {
         HB_PROF(0);
@@ -667,6 +786,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
                 }
                 __syncwarp();
                 r++;
+                if (pos < P.k) S.churn++;
                 if (pos < scan) scan = pos;
                 if (r > ef) {  // evict the maximum (d, id)
                     r = ef;
@@ -692,7 +812,12 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
         }
         if (vis_count > vis_lim) C.status |= ST_VISITED;
         if (C.status) break;
+        if (track && (++S.hops0 % STOP_EVERY) == 0 && stop_checkpoint(P, C, S, r, scan, W)) break;
         __syncwarp();
+    }
+    if (track && P.trace_feat && lane == 0) {
+        P.trace_count[C.q] = min(S.cp, P.trace_cap);
+        P.trace_hops[C.q] = S.hops0;
     }
 }
 
@@ -962,6 +1087,17 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
     C.Ad = reinterpret_cast<double *>(p);
     p += rerank ? al16(size_t(P.k + 1) * 8) : 0;
     C.Ai = reinterpret_cast<int32_t *>(p);
+    C.mlp_w = nullptr;
+    C.mlp_b = nullptr;
+    if (!FILT && P.stop_mlp) {  // block-shared copy of the network after the warp regions
+        unsigned char *m = smem + size_t(WPB) * wb;
+        const unsigned char *src = static_cast<const unsigned char *>(P.stop_mlp);
+        for (int i = threadIdx.x; i < int(MLP_BYTES / 4); i += blockDim.x)
+            reinterpret_cast<uint32_t *>(m)[i] = reinterpret_cast<const uint32_t *>(src)[i];
+        __syncthreads();
+        C.mlp_w = reinterpret_cast<const __nv_bfloat16 *>(m);
+        C.mlp_b = reinterpret_cast<const float *>(m + size_t(MLP_BF16) * 2);
+    }
     const int64_t slot = int64_t(blockIdx.x) * WPB + warp;
     C.vis = P.vis + slot * P.vis_stride;
     C.vbits = P.vbits + slot * P.vbits_stride;
@@ -998,6 +1134,14 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
         C.ndist = 0;
         C.nhops = 0;
         C.status = 0;
+        C.q = q;
+        if (!FILT && (P.stop_mlp || P.trace_feat)) {
+            double ss = 0.0;
+            for (int i = lane; i < dim; i += 32) ss += C.qd[i] * C.qd[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(FULL, ss, o);
+            C.qfeat = log1pf(float(ss));
+        }
         // Entry point, then greedy descent (ef = 1) through the upper layers.
         int32_t e0 = int32_t(P.entry_point);
         double d0 = dist_one<MODE, U8>(P, C, e0);
@@ -1287,7 +1431,10 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     const int krr = a->rerank_queries ? a->k : 0;
     const int s_cap = 256;
     const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr);
-    const size_t smem_block = wb * WPB;
+    const bool use_mlp = a->stop_mlp != nullptr && !filt;
+    const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
+    if (a->trace_feat && (!a->trace_dk || !a->trace_count || !a->trace_hops || a->trace_cap < 1))
+        return fail(HNSW_B200_EINVAL, "trace needs trace_dk, trace_count, trace_hops and trace_cap");
     if (smem_block > 227 * 1024)
         return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory (" +
                                           std::to_string(smem_block) + " bytes per block)");
@@ -1345,6 +1492,13 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.queue = ctr;
     P.n_failed = ctr + 1;
     P.s_cap = s_cap;
+    P.stop_mlp = use_mlp ? a->stop_mlp : nullptr;
+    P.stop_threshold = a->stop_threshold;
+    P.trace_feat = filt ? nullptr : a->trace_feat;
+    P.trace_dk = a->trace_dk;
+    P.trace_count = a->trace_count;
+    P.trace_hops = a->trace_hops;
+    P.trace_cap = a->trace_cap;
 
     int32_t n_work = nq;
     const int32_t *qlist = nullptr;

@@ -203,13 +203,18 @@ class DeviceGraph:
         dist_mode: int | None = None,
         counters: bool = True,
         out: tuple[torch.Tensor, ...] | None = None,
+        stop: tuple[torch.Tensor, float] | None = None,
+        trace: tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor] | None = None,
     ) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor | None]:
         """One batched search; returns device tensors ``(ids, dists, counters)``.
 
         ``queries``: (nq, dim) float32 prepared queries, or float64 code-space queries with
         ``use_codes``. ``ef``: scalar or (nq,) raw efSearch (layer 0 uses ``max(ef, k_search)``).
         ``allowed``: bool mask (n,) or a device uint32 bitmap. ``rerank_queries``: float32 prepared
-        queries for the fused exact re-rank of the first ``k_search`` beam entries.
+        queries for the fused exact re-rank of the first ``k_search`` beam entries. ``stop``:
+        ``(packed network, threshold)`` for the learned early termination; ``trace``: device
+        buffers ``(features (nq, cap, 12) f32, kth (nq, cap) f64, count (nq,) i32, hops (nq,) i32)``
+        filled with the stop features every 16 layer-0 expansions.
         """
         dev = self.device
         nq = int(queries.shape[0])
@@ -262,6 +267,13 @@ class DeviceGraph:
                 out_ids=_dev_ptr(ids),
                 out_dists=_dev_ptr(dists),
                 out_counters=_dev_ptr(ctr),
+                stop_mlp=_dev_ptr(stop[0]) if stop is not None else None,
+                stop_threshold=float(stop[1]) if stop is not None else 0.0,
+                trace_cap=int(trace[0].shape[1]) if trace is not None else 0,
+                trace_feat=_dev_ptr(trace[0]) if trace is not None else None,
+                trace_dk=_dev_ptr(trace[1]) if trace is not None else None,
+                trace_count=_dev_ptr(trace[2]) if trace is not None else None,
+                trace_hops=_dev_ptr(trace[3]) if trace is not None else None,
             )
             stream = torch.cuda.current_stream(dev).cuda_stream
             _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args), ctypes.c_void_p(stream)))

@@ -1,0 +1,79 @@
+"""Train the early-termination network for a workload graph.
+
+    python -m hnsw_engine_b200.train_stop --workload mix1m
+
+1. 200,000 training queries from the workload's generator (seed 2 for the mixture, 5 for the
+   Student-t data) are searched by the plain GPU kernel at the cap efSearch (512) with the trace on;
+2. the tensor-core exact k-NN gives each query's exact k-th distance; each checkpoint is labelled
+   with log1p(checkpoints remaining until the top-k is final);
+3. the network is trained with the library's CUDA forward/backward/Adam kernels;
+4. the stop threshold is tuned on 10,000 validation queries (seed 9) for recall@10 >= 0.95.
+
+The model is written to ``graphs/<workload>/stopnet/`` (git-ignored, next to the graph).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import graphs, synthetic
+from .exact_knn import exact_search
+from .index import HNSWIndex
+from .learned_stop import StopNetwork, collect_traces, label_traces, tune_threshold
+from .validation import prepare
+
+VALIDATION_SEED = 9
+
+
+def train(workload: str, n_train: int = 200_000, ef_cap: int = 512, k: int = 10,
+          target: float = 0.95, epochs: int = 4, n_val: int = 10_000, device: str = "cuda") -> dict:
+    t0 = time.time()
+    meta, arrays = graphs.open_workload(workload)
+    params = {kk: v for kk, v in meta["params"].items() if kk != "engine"}
+    metric = params["metric"]
+    index = HNSWIndex.from_arrays(arrays, int(meta["entry_point"]), int(meta["max_level"]),
+                                  device=device, **params)
+    g = index.device_graph
+    gen_seed = synthetic.TRAIN_SEED if graphs.WORKLOADS[workload]["gen"] == "mixture" else synthetic.T_TRAIN_SEED
+    q_train = prepare(graphs.workload_queries(workload, nq=n_train, seed=gen_seed), metric)
+    q_val = prepare(graphs.workload_queries(workload, nq=n_val, seed=VALIDATION_SEED), metric)
+    log = {"workload": workload, "n_train": n_train, "ef_cap": ef_cap, "k": k, "target": target}
+
+    tr = collect_traces(g, q_train, k, ef_cap)
+    t_tr = time.time()
+    _, true_d = exact_search(g.vectors, torch.from_numpy(q_train).to(g.device), k, metric)
+    true_kth = true_d[:, k - 1].cpu().numpy()
+    X, y, _ = label_traces(tr, true_kth)
+    log.update(trace_seconds=t_tr - t0, samples=int(X.shape[0]),
+               mean_checkpoints=float(tr.count.mean()), label_mean=float(y.mean()))
+
+    net = StopNetwork(g.device)
+    losses = net.fit(X, y, epochs=epochs)
+    log["epoch_losses"] = losses
+
+    _, val_d = exact_search(g.vectors, torch.from_numpy(q_val).to(g.device), k, metric)
+    thr, rec = tune_threshold(g, net, q_val, val_d.cpu().numpy(), k, ef_cap, target)
+    log.update(threshold=thr, validation_recall=rec, seconds=time.time() - t0)
+    out = graphs.graph_dir(workload) / "stopnet"
+    net.save(out)
+    (out / "train_log.json").write_text(json.dumps(log, indent=2))
+    return log
+
+
+def main() -> None:
+    p = argparse.ArgumentParser()
+    p.add_argument("--workload", default="mix1m")
+    p.add_argument("--n-train", type=int, default=200_000)
+    p.add_argument("--ef-cap", type=int, default=512)
+    p.add_argument("--epochs", type=int, default=4)
+    args = p.parse_args()
+    print(json.dumps(train(args.workload, args.n_train, args.ef_cap, epochs=args.epochs)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -93,7 +93,21 @@ typedef struct hnsw_b200_search_args {
     int64_t *out_ids;             /* (nq, k) int64, -1 padded */
     double *out_dists;            /* (nq, k) float64, +inf padded */
     int64_t *out_counters;        /* (nq, 2) int64 distance computations, hops; or NULL */
+    /* Learned early termination (unfiltered layer 0 only). Every HNSW_B200_STOP_EVERY layer-0
+     * expansions the kernel computes HNSW_B200_STOP_FEATURES search-progress features; with a
+     * network it stops the query once the prediction falls below stop_threshold. */
+    const void *stop_mlp;         /* packed network (hnsw_b200_mlp_pack layout), or NULL */
+    float stop_threshold;
+    int32_t trace_cap;            /* checkpoints per query in the trace buffers */
+    float *trace_feat;            /* (nq, trace_cap, HNSW_B200_STOP_FEATURES) features, or NULL */
+    double *trace_dk;             /* (nq, trace_cap) k-th result distance at each checkpoint */
+    int32_t *trace_count;         /* (nq,) checkpoints recorded */
+    int32_t *trace_hops;          /* (nq,) layer-0 expansions of the whole search */
 } hnsw_b200_search_args_t;
+
+#define HNSW_B200_STOP_EVERY 16
+#define HNSW_B200_STOP_FEATURES 12
+#define HNSW_B200_STOP_HIDDEN 64
 
 /* Element types of hnsw_b200_exact_knn inputs. */
 #define HNSW_B200_F32 0
@@ -123,6 +137,27 @@ typedef struct hnsw_b200_exact_args {
  * lower id). Replaces oracle.exact_search (src/hnsw_engine/oracle.py:35-126). Synchronises
  * `stream`. */
 int hnsw_b200_exact_knn(const hnsw_b200_exact_args_t *args, void *stream);
+
+/* ---- Early-termination network (no reference counterpart): 12 -> 64 -> 64 -> 1, ReLU.
+ * Master parameters are float32 in the order W1[64][12], b1[64], W2[64][64], b2[64], W3[64], b3;
+ * forward passes use BF16-rounded weights with FP32 accumulation, as the in-search inference. */
+int64_t hnsw_b200_mlp_param_count(void);
+int64_t hnsw_b200_mlp_packed_bytes(void);
+int64_t hnsw_b200_mlp_scratch_bytes(int32_t batch);
+/* One Adam step (step counts from 1) on a batch of (features, target) pairs; loss receives the
+ * batch mean squared error (device float). scratch: hnsw_b200_mlp_scratch_bytes(batch) bytes. */
+int hnsw_b200_mlp_train_step(float *params, float *adam_m, float *adam_v, int64_t step, float lr,
+                             const float *features, const float *targets, int32_t batch,
+                             float *scratch, float *loss, void *stream);
+/* Gradients of the batch mean squared error with respect to the parameters (no update). */
+int hnsw_b200_mlp_gradients(const float *params, const float *features, const float *targets,
+                            int32_t batch, float *scratch, float *grads, float *loss, void *stream);
+int hnsw_b200_mlp_predict(const float *params, const float *features, int64_t n, float *out,
+                          void *stream);
+/* Pack master parameters and the feature standardisation (mean, 1/std: 12 floats each, device)
+ * into the search kernel's layout (hnsw_b200_mlp_packed_bytes bytes). */
+int hnsw_b200_mlp_pack(const float *params, const float *mean, const float *inv_std, void *packed,
+                       void *stream);
 
 /* Create a search handle over a graph whose arrays live on the current CUDA device. */
 int hnsw_b200_open(const hnsw_b200_graph_t *graph, void **handle);

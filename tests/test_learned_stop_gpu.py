@@ -1,0 +1,154 @@
+"""CUDA training kernels against the NumPy oracle, in-search inference, and what the network gains."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import mlp
+
+pytestmark = pytest.mark.gpu
+
+
+def _net(seed=1):
+    import torch
+
+    from hnsw_engine_b200.learned_stop import StopNetwork
+
+    net = StopNetwork("cuda")
+    net.params = torch.from_numpy(mlp.init_params(seed)).cuda()
+    return net
+
+
+def test_cuda_gradients_match_oracle() -> None:
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((512, 12)).astype(np.float32)
+    y = rng.standard_normal(512).astype(np.float32)
+    net = _net()
+    g, loss = net.gradients(X, y)
+    p = net.params.cpu().numpy()
+    g_ref = mlp.gradients(p, X, y)
+    np.testing.assert_allclose(g, g_ref, rtol=2e-3, atol=2e-5)
+    assert loss == pytest.approx(mlp.loss(p, X, y), rel=1e-4)
+
+
+def test_cuda_predict_and_adam_match_oracle() -> None:
+    import torch
+
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((300, 12)).astype(np.float32)
+    y = rng.standard_normal(300).astype(np.float32)
+    net = _net(4)
+    p0 = net.params.cpu().numpy()
+    out = net.predict(X, normalize=False)
+    ref, _ = mlp.forward(p0, X)
+    np.testing.assert_allclose(out, ref, rtol=1e-4, atol=1e-5)
+    # one Adam step through the library vs the oracle's
+    from hnsw_engine_b200 import _lib
+
+    lib = _lib.load()
+    Xd, yd = torch.from_numpy(X).cuda(), torch.from_numpy(y).cuda()
+    scratch = torch.empty(int(lib.hnsw_b200_mlp_scratch_bytes(300)) // 4 + 1, device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.hnsw_b200_mlp_train_step(net.params.data_ptr(), net.m.data_ptr(), net.v.data_ptr(),
+                                            1, 1e-3, Xd.data_ptr(), yd.data_ptr(), 300,
+                                            scratch.data_ptr(), loss.data_ptr(), stream))
+    g_ref = mlp.gradients(p0, X, y)
+    p_ref, _, _ = mlp.adam_step(p0.astype(np.float64), 0, 0, g_ref, 1, 1e-3)
+    np.testing.assert_allclose(net.params.cpu().numpy(), p_ref, atol=2e-6)
+
+
+def test_training_reduces_loss() -> None:
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((40000, 12)).astype(np.float32)
+    y = (np.abs(X[:, 0]) + 0.5 * np.maximum(X[:, 1], 0) - 0.3 * X[:, 2]).astype(np.float32)
+    net = _net()
+    losses = net.fit(X, y, epochs=4, batch=256, lr=3e-3)
+    assert losses[-1] < 0.1 * float(np.var(y))
+    assert losses[-1] < losses[0]
+
+
+def _graph():
+    from hnsw_engine_b200 import HNSWIndex, graphs
+
+    name = "mix100k" if graphs.available("mix100k") else None
+    if name is None:
+        from conftest import mix10k_arrays
+
+        arrays, ep, ml = mix10k_arrays()
+        return HNSWIndex.from_arrays(arrays, ep, ml, dim=128, metric="l2", M=16).device_graph, "mix10k"
+    meta, arrays = graphs.open_workload(name)
+    params = {k: v for k, v in meta["params"].items() if k != "engine"}
+    return HNSWIndex.from_arrays(arrays, int(meta["entry_point"]), int(meta["max_level"]), **params).device_graph, name
+
+
+def test_in_kernel_inference_stops_where_the_network_says() -> None:
+    """A stopped search ends at the first checkpoint whose host-side prediction is below the
+    threshold (the trajectory up to there is the plain search's)."""
+    from hnsw_engine_b200 import graphs
+    from hnsw_engine_b200.learned_stop import collect_traces
+
+    g, name = _graph()
+    q = graphs.workload_queries(name, nq=500)
+    tr = collect_traces(g, q, 10, 256)
+    net = _net(7)
+    net.mean = tr.feat[tr.count > 0][:, 0].mean(0) * 0  # identity standardisation
+    X = tr.feat.reshape(-1, 12)
+    pred = net.predict(X, normalize=False).reshape(tr.feat.shape[:2])
+    thr = float(np.median(pred[:, 2]))
+    import torch
+
+    m = q.shape[0]
+    tf = torch.empty((m, 64, 12), device="cuda")
+    td = torch.empty((m, 64), dtype=torch.float64, device="cuda")
+    tc = torch.zeros(m, dtype=torch.int32, device="cuda")
+    th = torch.zeros(m, dtype=torch.int32, device="cuda")
+    g.search(q, 10, 256, stop=(net.packed(), thr), trace=(tf, td, tc, th))
+    stop_hops = th.cpu().numpy()
+    checked = 0
+    for i in range(m):
+        c = tr.count[i]
+        below = np.flatnonzero(pred[i, :c] < thr)
+        if below.size and np.all(np.abs(pred[i, : below[0] + 1] - thr) > 1e-4):
+            assert stop_hops[i] == 16 * (below[0] + 1), i
+            checked += 1
+        elif not below.size and np.all(np.abs(pred[i, :c] - thr) > 1e-4):
+            assert stop_hops[i] == tr.hops[i], i
+            checked += 1
+    assert checked > 0.9 * m
+
+
+def test_trained_network_beats_fixed_ef_at_equal_recall() -> None:
+    """On the same held-out queries and recall target, the learned stop computes fewer distances
+    than the smallest fixed efSearch that reaches the target."""
+    import torch
+
+    from hnsw_engine_b200 import graphs
+    from hnsw_engine_b200.exact_knn import exact_search
+    from hnsw_engine_b200.learned_stop import (StopNetwork, collect_traces, label_traces,
+                                               recall_of, tune_threshold)
+
+    g, name = _graph()
+    k, cap, target = 10, 256, 0.95
+    q_tr = graphs.workload_queries(name, nq=20000, seed=2)
+    q_ev = graphs.workload_queries(name, nq=2000, seed=1)
+    tr = collect_traces(g, q_tr, k, cap)
+    _, td = exact_search(g.vectors, torch.from_numpy(q_tr).cuda(), k, "l2")
+    X, y, _ = label_traces(tr, td[:, k - 1].cpu().numpy())
+    net = StopNetwork("cuda")
+    net.fit(X, y, epochs=4)
+    _, ev_d = exact_search(g.vectors, torch.from_numpy(q_ev).cuda(), k, "l2")
+    ev_d = ev_d.cpu().numpy()
+    thr, rec = tune_threshold(g, net, q_ev, ev_d, k, cap, target)
+    assert rec >= target
+    ids, d, ctr = g.search(q_ev, k, cap, stop=(net.packed(), thr))
+    learned_dists = int(ctr[:, 0].sum())
+    plain = None
+    for ef in (10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256):
+        ids, d, ctr = g.search(q_ev, k, ef)
+        if recall_of(ids.cpu().numpy(), d.cpu().numpy(), ev_d, k) >= target:
+            plain = int(ctr[:, 0].sum())
+            break
+    assert plain is not None
+    assert learned_dists < plain, (learned_dists, plain)
