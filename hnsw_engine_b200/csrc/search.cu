@@ -62,7 +62,11 @@ constexpr int WPB = 4;  // warps per block
 #define HB_NB_EXACT 4
 #endif
 #ifndef HB_NB_BYTES
-#define HB_NB_BYTES 16
+#define HB_NB_BYTES 8
+#endif
+// Layer-0 speculation: 0 off, 1 next candidate's links, 2 also L2 prefetch of its neighbours.
+#ifndef HB_SPECULATE
+#define HB_SPECULATE 0
 #endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
@@ -134,12 +138,13 @@ struct SearchParams {
     int32_t s_cap;
     // learned early termination (layer 0, unfiltered): features every STOP_EVERY expansions
     const void *stop_mlp;   // packed network (see mlp_smem_bytes), or NULL
-    float stop_threshold;   // stop once the predicted log1p(remaining checkpoints) falls below it
+    float stop_threshold;   // stop once the predicted further recall@k hits fall below it
     float *trace_feat;      // (n_queries, trace_cap, STOP_FEATURES) or NULL
-    double *trace_dk;       // (n_queries, trace_cap): k-th result distance at each checkpoint
+    double *trace_dk;       // (n_queries, trace_cap, trace_k): first results' distances per checkpoint
     int32_t *trace_count;   // (n_queries,) checkpoints recorded
     int32_t *trace_hops;    // (n_queries,) layer-0 expansions of the whole search
     int32_t trace_cap;
+    int32_t trace_k;        // distances recorded per checkpoint (min(k, 16))
 };
 
 constexpr int STOP_EVERY = 16;
@@ -204,6 +209,23 @@ __device__ __forceinline__ int count_below(const double *Ad, const int32_t *Ai, 
     int c = 0;
     for (int i = lane; i < m; i += 32) c += pair_lt(Ad[i], Ai[i] & ID_MASK, d, id);
     return __reduce_add_sync(FULL, c);
+}
+
+// Same as count_below for a sorted ascending array, by a two-level warp search: 32 splitters, then
+// the chunk that holds the boundary (exact for m <= 1024; falls back to the linear count beyond).
+__device__ __forceinline__ int sorted_rank(const double *Ad, const int32_t *Ai, int m, double d,
+                                           int32_t id, int lane) {
+    if (m > 1024) return count_below(Ad, Ai, m, d, id, lane);
+    const int step = (m + 31) >> 5;  // entries per chunk
+    const int s = lane * step;
+    const bool below = s < m && pair_lt(Ad[s], Ai[s] & ID_MASK, d, id);
+    const uint32_t b = __ballot_sync(FULL, below);  // chunks starting below (d, id): a prefix
+    const int chunks = __popc(b);
+    if (chunks == 0) return 0;
+    const int base = (chunks - 1) * step;  // the last chunk starting below holds the boundary
+    const int i = base + lane;
+    const bool in = lane < step && i < m && pair_lt(Ad[i], Ai[i] & ID_MASK, d, id);
+    return base + __popc(__ballot_sync(FULL, in));
 }
 
 // Entries of the descending array [0, m) strictly above (d, id).
@@ -658,6 +680,7 @@ struct StopState {
     int hops0;        // layer-0 expansions
     int churn;        // admissions into the first k results since the last checkpoint
     int cp;           // checkpoints taken
+    int stale;        // consecutive checkpoints without a change of the first k results
     float dk_prev, dk_prev2, d_entry;
 };
 
@@ -678,6 +701,10 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, S
             break;
         }
     }
+    // Unexpanded entries among the first k results (pending candidates that could still improve
+    // the top k), and stagnation of the first k.
+    const int unexp = __popc(__ballot_sync(FULL, lane < kk && !(C.Ri[min(lane, kk - 1)] & EXP_BIT)));
+    S.stale = S.churn == 0 ? S.stale + 1 : 0;
     float f[STOP_FEATURES];
     f[0] = d1;
     f[1] = dk;
@@ -686,16 +713,20 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, S
     f[4] = float(S.hops0) * (1.f / 64.f);
     f[5] = float(C.ndist) * (1.f / 1024.f);
     f[6] = S.d_entry;
-    f[7] = C.qfeat;
+    f[7] = float(unexp) / float(max(P.k, 1));
     f[8] = dk - S.d_entry;
-    f[9] = d1 - dk;
+    f[9] = float(S.stale) * 0.25f;
     f[10] = float(S.churn) * (1.f / STOP_EVERY);
     f[11] = log1pf(float(dn)) - dk;
-    if (P.trace_feat && S.cp < P.trace_cap && lane == 0) {
-        float *row = P.trace_feat + (int64_t(C.q) * P.trace_cap + S.cp) * STOP_FEATURES;
+    if (P.trace_feat && S.cp < P.trace_cap) {
+        if (lane == 0) {
+            float *row = P.trace_feat + (int64_t(C.q) * P.trace_cap + S.cp) * STOP_FEATURES;
 #pragma unroll
-        for (int i = 0; i < STOP_FEATURES; i++) row[i] = f[i];
-        P.trace_dk[int64_t(C.q) * P.trace_cap + S.cp] = C.Rd[kk - 1];
+            for (int i = 0; i < STOP_FEATURES; i++) row[i] = f[i];
+        }
+        if (lane < P.trace_k)
+            P.trace_dk[(int64_t(C.q) * P.trace_cap + S.cp) * P.trace_k + lane] =
+                lane < r ? C.Rd[lane] : INFINITY;
     }
     S.cp++;
     S.dk_prev2 = S.dk_prev;
@@ -725,7 +756,10 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
     int scan = 0;  // every result before `scan` is expanded
     int tn = 0;    // tie stack depth
     const bool track = layer == 0 && (P.trace_feat != nullptr || C.mlp_w != nullptr);
-    StopState S{0, 0, 0, 0.f, 0.f, log1pf(float(C.Rd[0]))};
+    // Speculation (layer 0): the links of the next unexpanded result are loaded while the current
+    // node is processed; they are used if that node is indeed popped next.
+    int32_t spec_c = -1, spec_cnt = 0, spec_e = -1;
+    StopState S{0, 0, 0, 0, 0.f, 0.f, log1pf(float(C.Rd[0]))};
     HB_PROF_DECL
     for (;;) {
         HB_PROF(0);
@@ -753,10 +787,38 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
         C.nhops++;
         HB_PROF(1);
         int cnt, stride;
-        const int32_t *nb = node_links(P, c, layer, cnt, stride);
+        const int32_t *nb;
+        int32_t e0;
+        if (c == spec_c) {  // loaded during the previous expansion
+            cnt = spec_cnt;
+            stride = P.links0_stride;
+            nb = P.links0 + int64_t(c) * P.links0_stride;
+            e0 = lane < cnt ? spec_e : -1;
+        } else {
+            nb = node_links(P, c, layer, cnt, stride);
+            e0 = first_link(nb, stride, cnt, lane);
+        }
+        if (layer == 0 && HB_SPECULATE) {
+            // Next guess: the first unexpanded result after the popped one (the tie stack's top if
+            // none); its count and first link chunk are loaded now, concurrently with this node.
+            int32_t c2 = -1;
+            for (int b0 = scan; b0 < r; b0 += 32) {
+                const int i = b0 + lane;
+                const uint32_t m = __ballot_sync(FULL, i < r && !(C.Ri[i] & EXP_BIT));
+                if (m) {
+                    c2 = C.Ri[b0 + __ffs(m) - 1];
+                    break;
+                }
+            }
+            if (c2 < 0 && tn > 0) c2 = C.ties[tn - 1];
+            spec_c = c2;
+            if (c2 >= 0) {
+                spec_cnt = __ldg(P.count0 + c2);
+                spec_e = lane < P.links0_stride ? __ldg(P.links0 + int64_t(c2) * P.links0_stride + lane) : -1;
+            }
+        }
         for (int base = 0; base < cnt; base += 32) {
-            const int32_t e = base == 0 ? first_link(nb, stride, cnt, lane)
-                                        : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
+            const int32_t e = base == 0 ? e0 : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
 #ifdef HB_PROFILE
             __syncwarp();
             if (__shfl_sync(FULL, e, 0) == -2) C.status |= 64;  // consume the load before timing
@@ -771,6 +833,15 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
 #endif
             HB_PROF(5);
             C.ndist += __popc(um);
+            if (layer == 0 && HB_SPECULATE >= 2 && base == 0 && spec_c >= 0 && lane < spec_cnt &&
+                spec_e >= 0) {
+                // Warm L2 with the guessed node's neighbours: their bitmap words and rows.
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(C.vbits + (spec_e >> 5)));
+                if (MODE == MODE_BYTES)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(P.rows8 + int64_t(spec_e) * P.dim));
+                else if (!U8)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(P.vectors + int64_t(spec_e) * P.dim));
+            }
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
                 const int j = __ffs(am) - 1;
@@ -778,7 +849,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
                 const double d = __shfl_sync(FULL, dj, j);
                 const int32_t id = __shfl_sync(FULL, e, j);
                 if (!(r < ef || d < W)) continue;  // uniform
-                const int pos = count_below(C.Rd, C.Ri, r, d, id, lane);
+                const int pos = sorted_rank(C.Rd, C.Ri, r, d, id, lane);
                 shift_up(C.Rd, C.Ri, pos, r, lane);
                 if (lane == 0) {
                     C.Rd[pos] = d;
@@ -1499,6 +1570,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.trace_count = a->trace_count;
     P.trace_hops = a->trace_hops;
     P.trace_cap = a->trace_cap;
+    P.trace_k = 16;
 
     int32_t n_work = nq;
     const int32_t *qlist = nullptr;

@@ -213,7 +213,8 @@ class DeviceGraph:
         ``allowed``: bool mask (n,) or a device uint32 bitmap. ``rerank_queries``: float32 prepared
         queries for the fused exact re-rank of the first ``k_search`` beam entries. ``stop``:
         ``(packed network, threshold)`` for the learned early termination; ``trace``: device
-        buffers ``(features (nq, cap, 12) f32, kth (nq, cap) f64, count (nq,) i32, hops (nq,) i32)``
+        buffers ``(features (nq, cap, 12) f32, first 16 result distances (nq, cap, 16) f64,
+        count (nq,) i32, hops (nq,) i32)``
         filled with the stop features every 16 layer-0 expansions.
         """
         dev = self.device

@@ -2,18 +2,19 @@
 
 Every 16 layer-0 expansions the search kernel computes 12 search-progress features (best and k-th
 result distances, the k-th distance's change over the last one and two checkpoints, expansions and
-distance computations so far, the layer-0 entry distance, the query norm, the k-th distance relative
-to the entry distance, best relative to k-th, how many admissions entered the first k results since
-the last checkpoint, and the frontier distance relative to the k-th). A 12 -> 64 -> 64 -> 1 ReLU
-network with BF16 weights predicts ``log1p(remaining checkpoints)`` until the query's top-k equals
-the exact oracle's (tie-aware, as ``recall_at_k``); the kernel stops a query once the prediction
-falls below a threshold tuned for the recall target.
+distance computations so far, the layer-0 entry distance, the share of the first k results not yet
+expanded, the k-th distance relative to the entry distance, checkpoints since the first k last
+changed, how many admissions entered the first k since the last checkpoint, and the frontier
+distance relative to the k-th). A 12 -> 64 -> 64 -> 1 ReLU network with BF16 weights predicts the
+recall@k hits (tie-aware, as ``recall_at_k``) that the query would still gain by searching on to the
+cap efSearch; the kernel stops a query once the predicted gain falls below a threshold tuned for the
+recall target.
 
 Pipeline (all GPU work in ``libhnsw_b200``):
 
 1. :func:`collect_traces` -- plain search at the cap efSearch with the trace buffers on;
 2. :func:`label_traces` -- the exact k-th distances (tensor-core exact k-NN) give, per checkpoint,
-   the remaining checkpoints until the top-k is final;
+   the hits the search would still gain;
 3. :class:`StopNetwork.fit` -- hand-written CUDA forward/backward/Adam (``hnsw_b200_mlp_*``);
 4. :func:`tune_threshold` -- bisection on a validation set for the recall target;
 5. search with ``stop_mlp`` / ``stop_threshold`` (``StopNetwork.packed``); the plain fixed-ef search
@@ -41,8 +42,8 @@ HIDDEN = 64
 STOP_EVERY = 16
 FEATURE_NAMES = (
     "log1p_d1", "log1p_dk", "dk_change_1", "dk_change_2", "hops_div64", "dists_div1024",
-    "log1p_d_entry", "log1p_qnorm2", "dk_minus_entry", "d1_minus_dk", "topk_churn",
-    "frontier_minus_dk",
+    "log1p_d_entry", "unexpanded_in_topk", "dk_minus_entry", "stale_checkpoints_div4",
+    "topk_churn", "frontier_minus_dk",
 )
 
 
@@ -58,10 +59,10 @@ def _stream(dev: torch.device) -> ctypes.c_void_p:
 @dataclass
 class Traces:
     feat: NDArray[np.float32]     # (nq, cap, 12)
-    dk: NDArray[np.float64]       # (nq, cap)
+    dk: NDArray[np.float64]       # (nq, cap, kt) first results' distances at each checkpoint
     count: NDArray[np.int32]      # (nq,) checkpoints recorded
     hops: NDArray[np.int32]       # (nq,) layer-0 expansions of the whole search
-    final_dk: NDArray[np.float64]  # (nq,) k-th distance returned by the full search
+    final_d: NDArray[np.float64]  # (nq, k) distances returned by the full search
 
 
 def collect_traces(graph: DeviceGraph, queries: Any, k: int, ef: int, trace_cap: int = 64,
@@ -70,15 +71,16 @@ def collect_traces(graph: DeviceGraph, queries: Any, k: int, ef: int, trace_cap:
     dev = graph.device
     nq = int(queries.shape[0])
     feat = np.empty((nq, trace_cap, FEATURES), np.float32)
-    dk = np.empty((nq, trace_cap), np.float64)
+    kt = 16  # the kernel records the first 16 result distances per checkpoint
+    dk = np.empty((nq, trace_cap, kt), np.float64)
     count = np.empty(nq, np.int32)
     hops = np.empty(nq, np.int32)
-    final = np.empty(nq, np.float64)
+    final = np.empty((nq, k), np.float64)
     for s in range(0, nq, chunk):
         e = min(nq, s + chunk)
         m = e - s
         tf = torch.empty((m, trace_cap, FEATURES), dtype=torch.float32, device=dev)
-        td = torch.empty((m, trace_cap), dtype=torch.float64, device=dev)
+        td = torch.empty((m, trace_cap, kt), dtype=torch.float64, device=dev)
         tc = torch.zeros(m, dtype=torch.int32, device=dev)
         th = torch.zeros(m, dtype=torch.int32, device=dev)
         _, dists, _ = graph.search(queries[s:e], k, ef, trace=(tf, td, tc, th))
@@ -86,27 +88,45 @@ def collect_traces(graph: DeviceGraph, queries: Any, k: int, ef: int, trace_cap:
         dk[s:e] = td.cpu().numpy()
         count[s:e] = tc.cpu().numpy()
         hops[s:e] = th.cpu().numpy()
-        final[s:e] = dists[:, k - 1].cpu().numpy()
+        final[s:e] = dists[:, :k].cpu().numpy()
     return Traces(feat, dk, count, hops, final)
 
 
-def label_traces(tr: Traces, true_kth: NDArray[np.float64]) -> tuple[NDArray, NDArray, NDArray]:
-    """Samples ``(X, y, qid)``: y = log1p(checkpoints remaining until the top-k is final).
+def checkpoint_hits(tr: Traces, true_kth: NDArray[np.float64]) -> tuple[NDArray, NDArray]:
+    """Tie-aware hits of the first k results at every checkpoint, and of the final result.
 
-    The top-k at a checkpoint is final when its k-th distance is within the tie-aware threshold of
-    the exact k-th distance (then every one of the k results counts for recall@k). A query that is
-    final only at the end of the search (or never) gets the remaining checkpoints to its end.
+    Results are unique and sorted, so a result counts exactly when its distance is within the
+    tie-aware threshold of the exact k-th distance (``recall_at_k``'s rule).
     """
     thr = true_kth + RELATIVE_TIE_TOLERANCE * np.maximum(1.0, np.abs(true_kth))
-    nq, cap = tr.dk.shape
+    k = tr.final_d.shape[1]
+    hits = (tr.dk[:, :, :k] <= thr[:, None, None]).sum(axis=2)
+    final = (tr.final_d <= thr[:, None]).sum(axis=1)
+    return hits, final
+
+
+def label_traces(tr: Traces, true_kth: NDArray[np.float64], target: str = "gain"
+                 ) -> tuple[NDArray, NDArray, NDArray]:
+    """Samples ``(X, y, qid)`` from every recorded checkpoint.
+
+    ``target="gain"`` (default): y = the recall@k hits the search would still add by running to its
+    end (the full search's tie-aware hits minus the checkpoint's); stopping where the predicted
+    gain is small trades the fewest hits for the most saved work, which is what an average recall
+    target rewards. ``target="remaining"``: y = log1p(checkpoints remaining until the result
+    reaches its final hits).
+    """
+    nq, cap = tr.dk.shape[:2]
     cps = np.arange(cap)[None, :]
     valid = cps < tr.count[:, None]
-    ok = valid & (tr.dk <= thr[:, None])
-    first = np.where(ok.any(axis=1), ok.argmax(axis=1), -1)
-    end_cp = tr.hops / STOP_EVERY  # the search ends after this many checkpoints (fractional)
-    target = np.where(first >= 0, first, np.maximum(end_cp, tr.count))
-    remaining = np.maximum(0.0, target[:, None] - cps)
-    y = np.log1p(remaining).astype(np.float32)
+    hits, final = checkpoint_hits(tr, true_kth)
+    if target == "gain":
+        y = np.maximum(0, final[:, None] - hits).astype(np.float32)
+    else:
+        ok = valid & (hits >= final[:, None])
+        first = np.where(ok.any(axis=1), ok.argmax(axis=1), -1)
+        end_cp = tr.hops / STOP_EVERY  # the search ends after this many checkpoints
+        last = np.where(first >= 0, first, np.maximum(end_cp, tr.count))
+        y = np.log1p(np.maximum(0.0, last[:, None] - cps)).astype(np.float32)
     X = tr.feat[valid]
     return X, y[valid], np.broadcast_to(np.arange(nq)[:, None], (nq, cap))[valid]
 
@@ -255,7 +275,7 @@ def tune_threshold(graph: DeviceGraph, net: StopNetwork, queries: Any, true_dist
                    ef: int, target: float, iters: int = 14) -> tuple[float, float]:
     """Largest threshold (earliest stops) whose measured recall@k on ``queries`` meets ``target``."""
     packed = net.packed()
-    lo, hi = -2.0, 4.0  # predictions are log1p(remaining checkpoints)
+    lo, hi = -1.0, 4.0  # predictions are expected further hits (0 .. k)
     best = (lo, 0.0)
     for _ in range(iters):
         mid = 0.5 * (lo + hi)

@@ -100,7 +100,8 @@ typedef struct hnsw_b200_search_args {
     float stop_threshold;
     int32_t trace_cap;            /* checkpoints per query in the trace buffers */
     float *trace_feat;            /* (nq, trace_cap, HNSW_B200_STOP_FEATURES) features, or NULL */
-    double *trace_dk;             /* (nq, trace_cap) k-th result distance at each checkpoint */
+    double *trace_dk;             /* (nq, trace_cap, 16) first 16 results' distances at each
+                                     checkpoint (+inf beyond the results held) */
     int32_t *trace_count;         /* (nq,) checkpoints recorded */
     int32_t *trace_hops;          /* (nq,) layer-0 expansions of the whole search */
 } hnsw_b200_search_args_t;

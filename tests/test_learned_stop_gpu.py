@@ -101,7 +101,7 @@ def test_in_kernel_inference_stops_where_the_network_says() -> None:
 
     m = q.shape[0]
     tf = torch.empty((m, 64, 12), device="cuda")
-    td = torch.empty((m, 64), dtype=torch.float64, device="cuda")
+    td = torch.empty((m, 64, 16), dtype=torch.float64, device="cuda")
     tc = torch.zeros(m, dtype=torch.int32, device="cuda")
     th = torch.zeros(m, dtype=torch.int32, device="cuda")
     g.search(q, 10, 256, stop=(net.packed(), thr), trace=(tf, td, tc, th))
@@ -136,6 +136,7 @@ def test_trained_network_beats_fixed_ef_at_equal_recall() -> None:
     tr = collect_traces(g, q_tr, k, cap)
     _, td = exact_search(g.vectors, torch.from_numpy(q_tr).cuda(), k, "l2")
     X, y, _ = label_traces(tr, td[:, k - 1].cpu().numpy())
+    assert np.isfinite(y).all() and (y >= 0).all()
     net = StopNetwork("cuda")
     net.fit(X, y, epochs=4)
     _, ev_d = exact_search(g.vectors, torch.from_numpy(q_ev).cuda(), k, "l2")
