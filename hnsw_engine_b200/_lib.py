@@ -113,6 +113,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                                ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_mlp_pack": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_void_p, ctypes.c_void_p]),
+    "hnsw_b200_search_noalloc": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.POINTER(SearchArgs),
+                                  ctypes.c_void_p]),
     "hnsw_b200_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
     "hnsw_b200_last_error": (ctypes.c_char_p, []),
     "hnsw_b200_version": (ctypes.c_char_p, []),

@@ -1357,6 +1357,17 @@ int launch_one(Handle &h, const SearchParams &P, size_t smem_block, int blocks, 
     return 0;
 }
 
+// Launch of the unfiltered kernel without a handle (the fixed-scratch entry point).
+template <int MODE, bool U8>
+int launch_one_noalloc(const SearchParams &P, size_t smem_block, int blocks, cudaStream_t s) {
+    auto kern = search_kernel<MODE, U8, false>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem_block)));
+    kern<<<blocks, WPB * 32, smem_block, s>>>(P);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 template <int MODE, bool U8>
 int launch_mode(Handle &h, const SearchParams &P, bool filt, size_t smem_block, int blocks,
                 cudaStream_t s) {
@@ -1639,3 +1650,195 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
 }
 
 }  // extern "C"
+
+// =========================================================================== fixed-scratch search
+// Some callers cannot allocate device memory at all: code running inside a CUDA-graph-captured
+// region or a real-time serving loop where an allocation would stall or be forbidden, plugins whose
+// host owns every device allocation through its own pool, and processes started under a hard device
+// memory budget. For them hnsw_b200_search_noalloc runs the same search kernel with all of its
+// working memory carved out of one fixed array that is part of the library image. The array is
+// HB_NOALLOC_BYTES (32 MiB) of device memory that every GPU which loads this library keeps until the
+// process exits, whether or not the entry point is used.
+namespace hb {
+
+constexpr size_t HB_NOALLOC_BYTES = size_t(32) << 20;
+constexpr int32_t HB_NOALLOC_MAX_NQ = 1 << 20;  // per-query status words live in the array too
+static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_BYTES];
+
+// Device address of g_noalloc_scratch, looked up once per device (the host-side symbol is only a
+// handle, not an address a kernel may use).
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[128] = {nullptr};
+
+int noalloc_scratch(void **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+        return fail(HNSW_B200_ECUDA, "search_noalloc: no current CUDA device");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(HNSW_B200_ECUDA, std::string("search_noalloc: cudaGetSymbolAddress failed: ") +
+                                             cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return 0;
+}
+
+}  // namespace hb
+
+extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
+                                        const hnsw_b200_search_args_t *a, void *stream) {
+    using namespace hb;
+    if (!graph || !a) return fail(HNSW_B200_EINVAL, "null argument");
+    const hnsw_b200_graph_t &g = *graph;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (g.n <= 0 || g.n > 0x7ffffffe || g.dim <= 0 || !g.vectors || !g.links0 || !g.count0 ||
+        !g.upper_offset || g.entry_point < 0 || g.entry_point >= g.n || g.metric < 0 || g.metric > 2)
+        return fail(HNSW_B200_EINVAL, "search_noalloc: invalid graph");
+    if (g.max_level > 0 && (!g.links_up || !g.count_up || g.rows <= 0))
+        return fail(HNSW_B200_EINVAL, "search_noalloc: upper layers need links_up and count_up");
+    if (a->allowed) return fail(HNSW_B200_EINVAL, "search_noalloc: filtered search needs hnsw_b200_search");
+    if (a->nq < 0) return fail(HNSW_B200_EINVAL, "nq out of range");
+    if (a->nq > HB_NOALLOC_MAX_NQ)
+        return fail(HNSW_B200_EINVAL, "search_noalloc: at most " + std::to_string(HB_NOALLOC_MAX_NQ) +
+                                          " queries per call (split the batch)");
+    if (a->nq == 0) return 0;
+    if (a->k < 1 || a->k_search < a->k) return fail(HNSW_B200_EINVAL, "need 1 <= k <= k_search");
+    if (!a->queries || !a->ef || !a->out_ids || !a->out_dists)
+        return fail(HNSW_B200_EINVAL, "queries, ef and outputs must be device pointers");
+    if (a->use_codes && !g.codes) return fail(HNSW_B200_EINVAL, "graph has no codes");
+    if (a->dist_mode < HNSW_B200_DIST_F64 || a->dist_mode > HNSW_B200_DIST_BYTES)
+        return fail(HNSW_B200_EINVAL, "unknown dist_mode");
+    if (a->dist_mode != HNSW_B200_DIST_F64 && g.metric == HNSW_B200_COSINE)
+        return fail(HNSW_B200_EINVAL, "exact integer modes need integer data (not cosine)");
+    const uint8_t *rows8 = a->use_codes ? g.codes : g.vector_bytes;
+    if (a->dist_mode == HNSW_B200_DIST_BYTES && (!rows8 || (g.dim & 3)))
+        return fail(HNSW_B200_EINVAL, "byte mode needs uint8 rows and dim a multiple of 4");
+    if (a->trace_feat && (!a->trace_dk || !a->trace_count || !a->trace_hops || a->trace_cap < 1))
+        return fail(HNSW_B200_EINVAL, "trace needs trace_dk, trace_count, trace_hops and trace_cap");
+    const bool u8 = a->use_codes != 0;
+    const int mode = a->dist_mode == HNSW_B200_DIST_BYTES
+                         ? MODE_BYTES
+                         : (a->dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64);
+    const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
+    const int krr = a->rerank_queries ? a->k : 0;
+    const size_t wb = warp_smem_bytes(ef_cap, g.dim, false, 256, krr);
+    const bool use_mlp = a->stop_mlp != nullptr;
+    const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
+    if (smem_block > 227 * 1024) return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory");
+    int bps = 0;
+    if (int rc = occupancy(mode, u8, false, smem_block, &bps)) return rc;
+    if (bps < 1) return fail(HNSW_B200_EINVAL, "search kernel cannot be resident");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+    // Carve the fixed array: counters, per-query status, then per warp slot the layer-0 bitmap, its
+    // list of marked ids, the upper-layer hash and the tie stack. The slot count is whatever fits.
+    void *base = nullptr;
+    if (int rc = noalloc_scratch(&base)) return rc;
+    const int32_t nq = int32_t(a->nq);
+    const int64_t vbits_stride = ((g.n + 31) / 32 + 3) / 4 * 4;
+    const int vlist_cap = int(std::min<int64_t>(65536, std::max<int64_t>(256, g.n / 256)));
+    const int vis_up_log2 = 10;
+    const int tie_cap = ef_cap + 64;
+    const size_t head = al16(4 * sizeof(int32_t)) + al16(size_t(nq) * sizeof(int32_t));
+    const size_t per_slot = size_t(vbits_stride) * 4 + al16(size_t(vlist_cap) * 4) +
+                            (size_t(1) << vis_up_log2) * 4 + al16(size_t(tie_cap) * 4);
+    if (head + per_slot * WPB > HB_NOALLOC_BYTES)
+        return fail(HNSW_B200_EINVAL, "search_noalloc: graph of " + std::to_string(g.n) +
+                                          " nodes needs more than the fixed " +
+                                          std::to_string(HB_NOALLOC_BYTES >> 20) + " MiB scratch");
+    const int64_t slot_fit = int64_t((HB_NOALLOC_BYTES - head) / per_slot) / WPB * WPB;
+    const int blocks = int(std::min<int64_t>(std::min<int64_t>(int64_t(sms) * bps, slot_fit / WPB),
+                                             (nq + WPB - 1) / WPB));
+    const int64_t slots = int64_t(blocks) * WPB;
+    unsigned char *p = static_cast<unsigned char *>(base);
+    int32_t *ctr = reinterpret_cast<int32_t *>(p);
+    int32_t *status = reinterpret_cast<int32_t *>(p + al16(4 * sizeof(int32_t)));
+    unsigned char *q = p + head;
+    uint32_t *vbits = reinterpret_cast<uint32_t *>(q);
+    q += size_t(slots) * vbits_stride * 4;
+    int32_t *vlist = reinterpret_cast<int32_t *>(q);
+    q += al16(size_t(slots) * vlist_cap * 4);
+    int32_t *vis = reinterpret_cast<int32_t *>(q);
+    q += size_t(slots) << vis_up_log2 << 2;
+    int32_t *ties = reinterpret_cast<int32_t *>(q);
+    // The array keeps the previous call's contents: zero the counters and the bitmaps (each
+    // query clears its own bits, but a previous call may have stopped part-way).
+    CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(int32_t), s));
+    CUDA_TRY(cudaMemsetAsync(vbits, 0, size_t(slots) * vbits_stride * 4, s));
+
+    SearchParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.vectors = g.vectors;
+    P.codes = g.codes;
+    P.rows8 = rows8;
+    P.links0 = g.links0;
+    P.count0 = g.count0;
+    P.upper_offset = g.upper_offset;
+    P.links_up = g.links_up;
+    P.count_up = g.count_up;
+    P.n = g.n;
+    P.dim = g.dim;
+    P.links0_stride = g.links0_stride;
+    P.links_up_stride = g.links_up_stride;
+    P.metric = g.metric;
+    P.entry_point = g.entry_point;
+    P.max_level = g.max_level;
+    P.queries = a->queries;
+    P.queries_f64 = a->queries_f64;
+    P.qlist = nullptr;
+    P.n_work = nq;
+    P.k = a->k;
+    P.k_search = a->k_search;
+    P.ef = a->ef;
+    P.ef_cap = ef_cap;
+    P.rerank_queries = a->rerank_queries;
+    P.out_ids = a->out_ids;
+    P.out_dists = a->out_dists;
+    P.out_ctr = a->out_counters;
+    P.status = status;
+    P.queue = ctr;
+    P.n_failed = ctr + 1;
+    P.vbits = vbits;
+    P.vbits_stride = vbits_stride;
+    P.vlist = vlist;
+    P.vlist_cap = vlist_cap;
+    P.vis = vis;
+    P.vis_stride = int64_t(1) << vis_up_log2;
+    P.vis_log2 = 0;
+    P.vis_up_log2 = vis_up_log2;
+    P.ties = ties;
+    P.tie_cap = tie_cap;
+    P.s_cap = 256;
+    P.stop_mlp = use_mlp ? a->stop_mlp : nullptr;
+    P.stop_threshold = a->stop_threshold;
+    P.trace_feat = a->trace_feat;
+    P.trace_dk = a->trace_dk;
+    P.trace_count = a->trace_count;
+    P.trace_hops = a->trace_hops;
+    P.trace_cap = a->trace_cap;
+    P.trace_k = 16;
+    int rc = 0;
+    if (mode == MODE_BYTES)
+        rc = launch_one_noalloc<MODE_BYTES, true>(P, smem_block, blocks, s);
+    else if (mode == MODE_EXACT)
+        rc = u8 ? launch_one_noalloc<MODE_EXACT, true>(P, smem_block, blocks, s)
+                : launch_one_noalloc<MODE_EXACT, false>(P, smem_block, blocks, s);
+    else
+        rc = u8 ? launch_one_noalloc<MODE_F64, true>(P, smem_block, blocks, s)
+                : launch_one_noalloc<MODE_F64, false>(P, smem_block, blocks, s);
+    if (rc) return rc;
+    int32_t failed = 0;  // pageable host copy: no pinned allocation either
+    CUDA_TRY(cudaMemcpyAsync(&failed, ctr + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (failed)
+        return fail(HNSW_B200_ERETRY, "search_noalloc: " + std::to_string(failed) +
+                                          " queries overflowed the fixed scratch (their outputs are "
+                                          "not written); search them with hnsw_b200_search");
+    return 0;
+}

@@ -171,6 +171,24 @@ void hnsw_b200_close(void *handle);
  * larger scratch; results are complete when it returns 0. */
 int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *args, void *stream);
 
+/* Batched search without any device allocation, for callers that are not allowed to allocate
+ * GPU memory: code inside CUDA-graph-captured or real-time serving loops, plugins whose host owns
+ * every device allocation, processes under a hard device-memory budget. No counterpart in the
+ * reference (its search runs on the CPU). It runs the same unfiltered search kernel as
+ * hnsw_b200_search, with all working memory taken from one fixed 32 MiB array inside the library
+ * image, which every GPU that loads the library holds until the process exits.
+ *   - limits: at most 1,048,576 queries per call; no filter; the graph's per-warp visited bitmap
+ *     (n / 8 bytes) must fit several times in the array, which bounds n at about 60 million
+ *     nodes; a query that outgrows its share returns HNSW_B200_ERETRY (use hnsw_b200_search);
+ *   - the first call on each device looks up the array's device address; make that first call
+ *     before any stream capture;
+ *   - every call uses the same array and leaves its contents behind (the counters and bitmaps are
+ *     cleared at the start of each call): calls that overlap on the GPU -- on two streams, or two
+ *     host threads -- race and must not be issued;
+ *   - it synchronises `stream` once to read the overflow count. */
+int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph, const hnsw_b200_search_args_t *args,
+                             void *stream);
+
 /* Number of device kernel launches made by the last hnsw_b200_search on this handle. */
 int64_t hnsw_b200_last_launches(void *handle);
 
