@@ -47,7 +47,7 @@ L2_BYTES = 126 * 1024 * 1024
 def parse() -> argparse.Namespace:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("b200", "reference"), default="b200")
     p.add_argument("--workload", default="mix1m")
@@ -211,6 +211,30 @@ def run_reference(args: argparse.Namespace) -> None:
 
 
 # ------------------------------------------------------------------------------------ GPU arm
+def timed_steps(step, steps: int, stream) -> list[float]:
+    """Per-step device milliseconds of ``steps`` calls of ``step`` (CUDA events on ``stream``)."""
+    import torch
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for i in range(steps):
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends, strict=True)]
+
+
+def max_over_ranks(pg, value: float, dev) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=dev, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -230,7 +254,9 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
-    from hnsw_engine_b200 import HNSWIndex, graphs
+    from hnsw_engine_b200 import HNSWIndex, graphs, synthetic
+    from hnsw_engine_b200.learned_stop import tune_threshold
+    from hnsw_engine_b200.train_stop import load_or_train
     from hnsw_engine_b200.validation import prepare
 
     meta, arrays = graphs.open_workload(args.workload)
@@ -243,98 +269,97 @@ def main() -> None:
     queries = prepare(raw_q, metric)
     nq, k = queries.shape[0], args.k
     dim = queries.shape[1]
-
-    # Exact ground truth and the plain fixed-ef operating point.
-    gt_ids, gt_d = ground_truth(g.vectors, queries, k, metric)
     q_dev = torch.from_numpy(queries).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    mode = g.choose_mode(queries, False)
+    row_bytes = dim * (1 if mode == 2 else 4)
+
+    # Exact ground truth; plain fixed-ef operating point: smallest efSearch reaching the target.
+    gt_ids, gt_d = ground_truth(g.vectors, queries, k, metric)
     sweep = {}
     ef_op = EF_LADDER[-1]
     for ef in EF_LADDER:
-        ids, dists, ctr = g.search(q_dev, k, ef)
-        rec = recall_of(ids.cpu().numpy(), dists.cpu().numpy(), gt_ids, gt_d, k)
-        sweep[ef] = rec
-        if rec >= RECALL_TARGET:
+        ids, dists, _ = g.search(q_dev, k, ef, dist_mode=mode)
+        sweep[ef] = recall_of(ids.cpu().numpy(), dists.cpu().numpy(), gt_ids, gt_d, k)
+        if sweep[ef] >= RECALL_TARGET:
             ef_op = ef
             break
     if rank == 0:
-        op_path = ROOT / "graphs" / args.workload / "operating_point.json"
         try:
-            op_path.write_text(json.dumps({"ef": ef_op, "recall": sweep[ef_op]}))
+            (ROOT / "graphs" / args.workload / "operating_point.json").write_text(
+                json.dumps({"ef": ef_op, "recall": sweep[ef_op]}))
         except OSError:
             pass
+
+    # Learned stop: the trained network (trained now if none is stored), its threshold tuned on
+    # the same queries for the same recall target (equal measured recall).
+    net = load_or_train(args.workload, device=str(dev))
+    cap = net.ef_cap
+    val_threshold = net.threshold
+    thr, _ = tune_threshold(g, net, q_dev, gt_d, k, cap, RECALL_TARGET)
+    packed = net.packed()
 
     ids_o = torch.empty((nq, k), dtype=torch.int64, device=dev)
     d_o = torch.empty((nq, k), dtype=torch.float64, device=dev)
     c_o = torch.empty((nq, 2), dtype=torch.int64, device=dev)
-    mode = g.choose_mode(queries, False)
-    stream = torch.cuda.current_stream(dev)
+    ids_p = torch.empty_like(ids_o)
+    d_p = torch.empty_like(d_o)
+    c_p = torch.empty_like(c_o)
 
-    def step():
-        g.search(q_dev, k, ef_op, out=(ids_o, d_o, c_o), dist_mode=mode)
+    def step_learned():
+        g.search(q_dev, k, cap, out=(ids_o, d_o, c_o), dist_mode=mode, stop=(packed, thr))
+
+    def step_plain():
+        g.search(q_dev, k, ef_op, out=(ids_p, d_p, c_p), dist_mode=mode)
 
     for _ in range(max(3, args.warmup)):
-        step()
+        step_learned()
+        step_plain()
     torch.cuda.synchronize()
     launches_per_step = g.last_launches
-    counters = c_o.cpu().numpy()
-    row_bytes = dim * (1 if mode == 2 else 4)
-    alg_bytes = algorithmic_bytes(counters, arrays, dim, k, row_bytes)
+    alg_bytes = algorithmic_bytes(c_o.cpu().numpy(), arrays, dim, k, row_bytes)
+    alg_bytes_plain = algorithmic_bytes(c_p.cpu().numpy(), arrays, dim, k, row_bytes)
 
-    # Device-resident timed region.
+    # Timed regions (device-resident inputs; graph and rows exceed L2, no flush needed).
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(local) as clocks:
-        for i in range(args.steps):
-            starts[i].record(stream)
-            step()
-            ends[i].record(stream)
-        torch.cuda.synchronize()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends, strict=True)]
-    total_ms = float(sum(step_ms))
-    if pg is not None:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
-        pg.barrier()
-    value = world * nq * args.steps / (total_ms / 1000.0)
-    mean_ms = total_ms / args.steps
-    rec_op = recall_of(ids_o.cpu().numpy(), d_o.cpu().numpy(), gt_ids, gt_d, k)
+        ms_learned = timed_steps(step_learned, args.steps, stream)
+        ms_plain = timed_steps(step_plain, args.steps, stream)
+    total_l = max_over_ranks(pg, float(sum(ms_learned)), dev)
+    total_p = max_over_ranks(pg, float(sum(ms_plain)), dev)
+    value = world * nq * args.steps / (total_l / 1000.0)
+    plain_qps = world * nq * args.steps / (total_p / 1000.0)
+    mean_ms = total_l / args.steps
+    rec_l = recall_of(ids_o.cpu().numpy(), d_o.cpu().numpy(), gt_ids, gt_d, k)
+    rec_p = recall_of(ids_p.cpu().numpy(), d_p.cpu().numpy(), gt_ids, gt_d, k)
+    hops_l = float(c_o[:, 1].float().mean())
+    hops_p = float(c_p[:, 1].float().mean())
 
-    # End to end through the public API with host buffers.
-    index.batch_search(raw_q, k=k, ef=ef_op)  # warm
+    # End to end through the public API with host buffers (numpy in, numpy out).
+    net.threshold = thr
+    index.batch_search(raw_q, k=k, ef=cap, stop=net)
     torch.cuda.synchronize()
     e_ms = []
     for _ in range(max(2, min(args.steps, 5))):
         t0 = time.perf_counter()
-        e_ids, e_d = index.batch_search(raw_q, k=k, ef=ef_op)
+        e_ids, e_d = index.batch_search(raw_q, k=k, ef=cap, stop=net)
         torch.cuda.synchronize()
         e_ms.append((time.perf_counter() - t0) * 1000.0)
-    e2e_ms = float(np.median(e_ms))
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(pg, float(np.median(e_ms)), dev)
     e2e_value = world * nq / (e2e_ms / 1000.0)
     assert np.array_equal(e_ids, ids_o.cpu().numpy()), "e2e results differ from device results"
 
     # Per-query efSearch uniform on 32..512 (the batched-at-scale configuration).
-    from hnsw_engine_b200 import synthetic
-
     pq = synthetic.per_query_ef(nq, seed=11, low=32, high=512)
     pq_dev = torch.from_numpy(pq).to(dev)
     g.search(q_dev, k, pq_dev, dist_mode=mode)
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
+    pq_ms = timed_steps(lambda: g.search(q_dev, k, pq_dev, dist_mode=mode), 3, stream)
     pq_ids, pq_d, pq_c = g.search(q_dev, k, pq_dev, dist_mode=mode)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    pq_ms = ev0.elapsed_time(ev1)
     pq_rec = recall_of(pq_ids.cpu().numpy(), pq_d.cpu().numpy(), gt_ids, gt_d, k)
     pq_bytes = algorithmic_bytes(pq_c.cpu().numpy(), arrays, dim, k, row_bytes)
+    pq_mean = float(np.median(pq_ms))
 
     pk = peaks()
     achieved = alg_bytes / (mean_ms / 1000.0) / 1e9
@@ -359,17 +384,24 @@ def main() -> None:
             "dtype": {2: "u8 (exact int32 dp4a)", 1: "f32 (exact integer)", 0: "f64"}[mode],
             "data": "synthetic",
             "config": {
-                "workload": f"{args.workload}: {arrays['vectors'].shape[0]} x {dim} integer mixture, "
-                            f"{metric}, M={params['M']}, efC={params['ef_construction']}, nq={nq}, k={k}",
-                "method": "plain fixed-ef",
-                "ef": ef_op,
-                "recall_at_10": rec_op,
+                "workload": f"{args.workload}: {arrays['vectors'].shape[0]} x {dim} "
+                            f"{graphs.WORKLOADS[args.workload]['gen']} data, {metric}, "
+                            f"M={params['M']}, efC={params['ef_construction']}, nq={nq}, k={k}",
+                "method": "learned stop (value) vs plain fixed-ef, equal recall target "
+                          f"{RECALL_TARGET}",
+                "learned_stop": {"ef_cap": cap, "threshold": thr, "recall_at_10": rec_l,
+                                 "qps": value, "mean_hops": hops_l,
+                                 "validation_threshold": val_threshold},
+                "plain_fixed_ef": {"ef": ef_op, "recall_at_10": rec_p, "qps": plain_qps,
+                                   "mean_hops": hops_p,
+                                   "achieved_gbs": alg_bytes_plain / (total_p / args.steps / 1000.0) / 1e9},
+                "learned_over_plain": value / plain_qps,
                 "ef_sweep": {str(e): r for e, r in sweep.items()},
                 "l2_policy": "inputs larger than L2 (vectors %d MB + links %d MB > 126 MB)"
                              % (arrays["vectors"].nbytes >> 20, np.asarray(arrays["links0"]).nbytes >> 20),
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                "per_query_ef_32_512": {"qps": world * nq / (pq_ms / 1000.0), "recall_at_10": pq_rec,
-                                        "achieved_gbs": pq_bytes / (pq_ms / 1000.0) / 1e9},
+                "per_query_ef_32_512": {"qps": world * nq / (pq_mean / 1000.0), "recall_at_10": pq_rec,
+                                        "achieved_gbs": pq_bytes / (pq_mean / 1000.0) / 1e9},
             },
             "roofline": {
                 "bound": "hbm",
@@ -380,6 +412,7 @@ def main() -> None:
                 "traffic": None,
                 "peak_source": pk["source"],
                 "algorithmic_bytes_per_launch": alg_bytes,
+                "row_bytes": row_bytes,
             },
             "cpu_baseline": cpu_base,
             "e2e": {

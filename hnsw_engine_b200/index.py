@@ -293,12 +293,15 @@ class HNSWIndex:
         return ids[0], dists[0]
 
     def batch_search(
-        self, queries: Any, k: int = 10, ef: Any = None, filter: ArrayLike | None = None
+        self, queries: Any, k: int = 10, ef: Any = None, filter: ArrayLike | None = None,
+        stop: Any = None,
     ) -> tuple[Any, Any]:
         """:meth:`search` for each row of ``(nq, dim)`` queries (reference ``index.py:275-292``).
 
         ``ef`` may be one integer or an array of one efSearch per query. Torch device queries give
-        device results (no host round trip); host queries give numpy results.
+        device results (no host round trip); host queries give numpy results. Extension: ``stop``,
+        a trained :class:`~hnsw_engine_b200.learned_stop.StopNetwork`, ends each unfiltered query
+        early once the network predicts no further recall gain (``ef`` is then the cap).
         """
         k_valid, ef_valid = self._check_search_args(k, ef)
         allowed = self._check_filter(filter)
@@ -319,13 +322,21 @@ class HNSWIndex:
             if on_device:
                 return torch.from_numpy(ids).to(queries.device), torch.from_numpy(dists).to(queries.device)
             return ids, dists
-        ids_t, dists_t = self._run(prepared, k_valid, ef_valid, allowed, keep_device=on_device)
+        ids_t, dists_t = self._run(prepared, k_valid, ef_valid, allowed, keep_device=on_device,
+                                   stop=stop)
         return ids_t, dists_t
 
     def _run(self, prepared: Any, k: int, ef: Any, allowed: NDArray[np.bool_] | None,
-             keep_device: bool = False) -> tuple[Any, Any]:
+             keep_device: bool = False, stop: Any = None) -> tuple[Any, Any]:
         g = self.device_graph
-        ids, dists, ctr = g.search(prepared, k, ef, allowed=allowed)
+        stop_arg = None
+        if stop is not None and allowed is None:
+            packed = getattr(stop, "_packed_cache", None)
+            if packed is None:
+                packed = stop.packed()
+                stop._packed_cache = packed
+            stop_arg = (packed, stop.threshold)
+        ids, dists, ctr = g.search(prepared, k, ef, allowed=allowed, stop=stop_arg)
         self._accumulate(ctr)
         if keep_device:
             return ids, dists

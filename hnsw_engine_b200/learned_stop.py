@@ -159,6 +159,7 @@ class StopNetwork:
         self.mean = np.zeros(FEATURES, np.float32)
         self.std = np.ones(FEATURES, np.float32)
         self.threshold = 0.0
+        self.ef_cap = 256
         self.history: list[float] = []
 
     def _norm(self, X: NDArray) -> NDArray[np.float32]:
@@ -240,8 +241,8 @@ class StopNetwork:
         np.save(root / "mean.npy", self.mean)
         np.save(root / "std.npy", self.std)
         (root / "meta.json").write_text(json.dumps({
-            "step": self.step, "threshold": self.threshold, "history": self.history,
-            "features": FEATURE_NAMES, "stop_every": STOP_EVERY,
+            "step": self.step, "threshold": self.threshold, "ef_cap": self.ef_cap,
+            "history": self.history, "features": FEATURE_NAMES, "stop_every": STOP_EVERY,
         }, indent=2))
 
     @classmethod
@@ -254,7 +255,10 @@ class StopNetwork:
         net.mean = np.load(root / "mean.npy")
         net.std = np.load(root / "std.npy")
         meta = json.loads((root / "meta.json").read_text())
+        if tuple(meta.get("features", ())) != FEATURE_NAMES:
+            raise ValueError(f"{root}: network trained on different stop features")
         net.step, net.threshold, net.history = meta["step"], meta["threshold"], meta["history"]
+        net.ef_cap = int(meta.get("ef_cap", 256))
         return net
 
 

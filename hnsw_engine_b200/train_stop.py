@@ -3,9 +3,9 @@
     python -m hnsw_engine_b200.train_stop --workload mix1m
 
 1. 200,000 training queries from the workload's generator (seed 2 for the mixture, 5 for the
-   Student-t data) are searched by the plain GPU kernel at the cap efSearch (512) with the trace on;
+   Student-t data) are searched by the plain GPU kernel at the cap efSearch (256) with the trace on;
 2. the tensor-core exact k-NN gives each query's exact k-th distance; each checkpoint is labelled
-   with log1p(checkpoints remaining until the top-k is final);
+   with the recall@10 hits the search would still gain by running to the cap;
 3. the network is trained with the library's CUDA forward/backward/Adam kernels;
 4. the stop threshold is tuned on 10,000 validation queries (seed 9) for recall@10 >= 0.95.
 
@@ -30,7 +30,7 @@ from .validation import prepare
 VALIDATION_SEED = 9
 
 
-def train(workload: str, n_train: int = 200_000, ef_cap: int = 512, k: int = 10,
+def train(workload: str, n_train: int = 200_000, ef_cap: int = 256, k: int = 10,
           target: float = 0.95, epochs: int = 4, n_val: int = 10_000, device: str = "cuda") -> dict:
     t0 = time.time()
     meta, arrays = graphs.open_workload(workload)
@@ -53,6 +53,7 @@ def train(workload: str, n_train: int = 200_000, ef_cap: int = 512, k: int = 10,
                mean_checkpoints=float(tr.count.mean()), label_mean=float(y.mean()))
 
     net = StopNetwork(g.device)
+    net.ef_cap = ef_cap
     losses = net.fit(X, y, epochs=epochs)
     log["epoch_losses"] = losses
 
@@ -65,11 +66,21 @@ def train(workload: str, n_train: int = 200_000, ef_cap: int = 512, k: int = 10,
     return log
 
 
+def load_or_train(workload: str, device: str = "cuda") -> StopNetwork:
+    """The workload's trained network (trained now, about 20 s on a B200, if none is stored)."""
+    path = graphs.graph_dir(workload) / "stopnet"
+    try:
+        return StopNetwork.load(path, device)
+    except (FileNotFoundError, ValueError, KeyError):
+        train(workload, device=device)
+        return StopNetwork.load(path, device)
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--workload", default="mix1m")
     p.add_argument("--n-train", type=int, default=200_000)
-    p.add_argument("--ef-cap", type=int, default=512)
+    p.add_argument("--ef-cap", type=int, default=256)
     p.add_argument("--epochs", type=int, default=4)
     args = p.parse_args()
     print(json.dumps(train(args.workload, args.n_train, args.ef_cap, epochs=args.epochs)), flush=True)
