@@ -56,13 +56,25 @@ def _generate(gen: str, n: int, dim: int, seed: int) -> NDArray[np.float32]:
 
 
 def workload_vectors(name: str) -> NDArray[np.float32]:
-    """The workload's data rows (float32, as the reference stores them after ``prepare``)."""
+    """The workload's data rows as handed to the reference's ``HNSWIndex.add`` by the build.
+
+    For cosine workloads the generator's rows are normalised once more here (float64, then cast),
+    so the data given to the build is already unit-length; the reference's ``prepare`` then
+    normalises again when it stores them (:func:`stored_vectors`).
+    """
     spec = WORKLOADS[name]
     x = _generate(spec["gen"], spec["n"], spec["dim"], spec["data_seed"])
     if spec["metric"] == "cosine":  # metrics.prepare: float64 normalise then cast
         x64 = x.astype(np.float64)
         x = np.ascontiguousarray(x64 / np.linalg.norm(x64, axis=1)[:, None], dtype=np.float32)
     return x
+
+
+def stored_vectors(name: str) -> NDArray[np.float32]:
+    """The rows the built graph holds: the reference's ``prepare`` of :func:`workload_vectors`."""
+    from .validation import prepare
+
+    return prepare(workload_vectors(name), WORKLOADS[name]["metric"])
 
 
 def workload_queries(name: str, nq: int | None = None, seed: int | None = None) -> NDArray[np.float32]:
@@ -94,7 +106,7 @@ def open_workload(name: str, mmap: bool = True) -> tuple[dict[str, Any], dict[st
     for array_name, expected in meta["arrays"].items():
         path = root / f"{array_name}.npy"
         if array_name == "vectors" and not path.is_file():
-            vec = workload_vectors(name)
+            vec = stored_vectors(name)
             digest = hashlib.sha256(vec.tobytes()).hexdigest()
             want = (root / "vectors.sha256").read_text().strip()
             if digest != want:

@@ -172,3 +172,16 @@ def test_large_graph_codes_cosine_match_oracle() -> None:
     codes = quant.encode(arrays["vectors"])
     q = quant.transform_queries(prepare(graphs.workload_queries("t100k", nq=200), metric), metric)
     _oracle_compare(arrays, ep, ml, metric, q, 10, 128, codes=codes)
+
+
+@pytest.mark.parametrize("name", ["mix1m", "t1m"])
+def test_million_node_graphs_match_oracle(name: str) -> None:
+    """The 1M-node workloads (integer L2 and float cosine): ids, distances and counters equal the
+    CPU oracle's for a sample of queries at per-query efSearch in 32..512."""
+    from hnsw_engine_b200 import graphs, synthetic
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload(name)
+    q = prepare(graphs.workload_queries(name, nq=96), metric)
+    ef = synthetic.per_query_ef(96, seed=6, low=32, high=512)
+    _oracle_compare(arrays, ep, ml, metric, q, 10, ef)
