@@ -134,6 +134,19 @@ def algorithmic_bytes(counters: np.ndarray, arrays: dict, dim: int, k: int, row_
     return dist * row_bytes + hops * (4.0 + 4.0 * mean_links) + nq * (dim * 4.0 + k * 16.0)
 
 
+def measured_traffic(workload: str) -> int | None:
+    """DRAM bytes (read + write) of one learned-stop search launch of this workload, as an ncu
+    capture of this same command recorded them (``profiles/search_kernel_bytes_<workload>.md``,
+    line ``traffic_bytes_per_launch: N``); None when no capture of the workload is committed."""
+    path = ROOT / "profiles" / f"search_kernel_bytes_{workload}.md"
+    if not path.is_file():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return int(line.split(":", 1)[1])
+    return None
+
+
 def ground_truth(vectors_dev, queries: np.ndarray, k: int, metric: str):
     """Exact top-k (ids, float64 distances) from the tensor-core exact k-NN (untimed)."""
     import torch
@@ -409,7 +422,9 @@ def main() -> None:
                 "peak": pk["hbm_gbs"],
                 "unit": "GB/s",
                 "frac": achieved / pk["hbm_gbs"],
-                "traffic": None,
+                "traffic": measured_traffic(args.workload),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one learned-stop "
+                                  "launch of this command (profiles/search_kernel_bytes_%s.md)" % args.workload,
                 "peak_source": pk["source"],
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "row_bytes": row_bytes,

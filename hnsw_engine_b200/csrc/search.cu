@@ -1588,7 +1588,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     for (int attempt = 0; attempt < 6; attempt++) {
         const int blocks = int(std::min<int64_t>(int64_t(h.sms) * bps, (n_work + WPB - 1) / WPB));
         const int64_t slots = int64_t(blocks) * WPB;
-        const int64_t vis_stride = int64_t(1) << std::max(vis_log2, vis_up_log2);
+        const int64_t vis_stride = int64_t(1) << vis_up_log2;  // layer 0 uses the bitmap
         if (int rc = h.vis.ensure(size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
         if (h.bits_dirty && h.vbits.ptr) {
             CUDA_TRY(cudaMemsetAsync(h.vbits.ptr, 0, h.vbits.bytes, s));

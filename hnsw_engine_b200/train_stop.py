@@ -3,7 +3,7 @@
     python -m hnsw_engine_b200.train_stop --workload mix1m
 
 1. 200,000 training queries from the workload's generator (seed 2 for the mixture, 5 for the
-   Student-t data) are searched by the plain GPU kernel at the cap efSearch (256) with the trace on;
+   Student-t data) are searched by the plain GPU kernel at the cap efSearch (192) with the trace on;
 2. the tensor-core exact k-NN gives each query's exact k-th distance; each checkpoint is labelled
    with the recall@10 hits the search would still gain by running to the cap;
 3. the network is trained with the library's CUDA forward/backward/Adam kernels;
@@ -30,7 +30,7 @@ from .validation import prepare
 VALIDATION_SEED = 9
 
 
-def train(workload: str, n_train: int = 200_000, ef_cap: int = 256, k: int = 10,
+def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
           target: float = 0.95, epochs: int = 4, n_val: int = 10_000, device: str = "cuda") -> dict:
     t0 = time.time()
     meta, arrays = graphs.open_workload(workload)
@@ -80,7 +80,7 @@ def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--workload", default="mix1m")
     p.add_argument("--n-train", type=int, default=200_000)
-    p.add_argument("--ef-cap", type=int, default=256)
+    p.add_argument("--ef-cap", type=int, default=192)
     p.add_argument("--epochs", type=int, default=4)
     args = p.parse_args()
     print(json.dumps(train(args.workload, args.n_train, args.ef_cap, epochs=args.epochs)), flush=True)
