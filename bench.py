@@ -59,11 +59,8 @@ def parse() -> argparse.Namespace:
 
 
 # ----------------------------------------------------------------------------------- helpers
-def dist_env() -> tuple[int, int, int]:
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+from hnsw_engine_b200.replicas import job_throughput, max_over_ranks  # noqa: E402
+from hnsw_engine_b200.replicas import rank_env as dist_env  # noqa: E402
 
 
 def peaks() -> dict:
@@ -238,16 +235,6 @@ def timed_steps(step, steps: int, stream) -> list[float]:
     return [a.elapsed_time(b) for a, b in zip(starts, ends, strict=True)]
 
 
-def max_over_ranks(pg, value: float, dev) -> float:
-    if pg is None:
-        return value
-    import torch
-
-    t = torch.tensor([value], device=dev, dtype=torch.float64)
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
-
-
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -342,8 +329,8 @@ def main() -> None:
         ms_plain = timed_steps(step_plain, args.steps, stream)
     total_l = max_over_ranks(pg, float(sum(ms_learned)), dev)
     total_p = max_over_ranks(pg, float(sum(ms_plain)), dev)
-    value = world * nq * args.steps / (total_l / 1000.0)
-    plain_qps = world * nq * args.steps / (total_p / 1000.0)
+    value = job_throughput(world, nq, args.steps, total_l)
+    plain_qps = job_throughput(world, nq, args.steps, total_p)
     mean_ms = total_l / args.steps
     rec_l = recall_of(ids_o.cpu().numpy(), d_o.cpu().numpy(), gt_ids, gt_d, k)
     rec_p = recall_of(ids_p.cpu().numpy(), d_p.cpu().numpy(), gt_ids, gt_d, k)
@@ -361,7 +348,7 @@ def main() -> None:
         torch.cuda.synchronize()
         e_ms.append((time.perf_counter() - t0) * 1000.0)
     e2e_ms = max_over_ranks(pg, float(np.median(e_ms)), dev)
-    e2e_value = world * nq / (e2e_ms / 1000.0)
+    e2e_value = job_throughput(world, nq, 1, e2e_ms)
     assert np.array_equal(e_ids, ids_o.cpu().numpy()), "e2e results differ from device results"
 
     # Per-query efSearch uniform on 32..512 (the batched-at-scale configuration).
@@ -372,7 +359,7 @@ def main() -> None:
     pq_ids, pq_d, pq_c = g.search(q_dev, k, pq_dev, dist_mode=mode)
     pq_rec = recall_of(pq_ids.cpu().numpy(), pq_d.cpu().numpy(), gt_ids, gt_d, k)
     pq_bytes = algorithmic_bytes(pq_c.cpu().numpy(), arrays, dim, k, row_bytes)
-    pq_mean = float(np.median(pq_ms))
+    pq_mean = max_over_ranks(pg, float(np.median(pq_ms)), dev)
 
     pk = peaks()
     achieved = alg_bytes / (mean_ms / 1000.0) / 1e9
@@ -413,7 +400,7 @@ def main() -> None:
                 "l2_policy": "inputs larger than L2 (vectors %d MB + links %d MB > 126 MB)"
                              % (arrays["vectors"].nbytes >> 20, np.asarray(arrays["links0"]).nbytes >> 20),
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                "per_query_ef_32_512": {"qps": world * nq / (pq_mean / 1000.0), "recall_at_10": pq_rec,
+                "per_query_ef_32_512": {"qps": job_throughput(world, nq, 1, pq_mean), "recall_at_10": pq_rec,
                                         "achieved_gbs": pq_bytes / (pq_mean / 1000.0) / 1e9},
             },
             "roofline": {

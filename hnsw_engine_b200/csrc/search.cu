@@ -68,6 +68,10 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_SPECULATE
 #define HB_SPECULATE 0
 #endif
+// Byte rows of at most 128 bytes: one lane per neighbour, row loads issued before the visited marks.
+#ifndef HB_LANE_ROWS
+#define HB_LANE_ROWS 1
+#endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
 #define HB_PROF_DECL unsigned long long hb_t = clock64();
@@ -193,6 +197,7 @@ struct Ctx {
     long long ndist, nhops;  // uniform across the warp
     int32_t status;          // uniform across the warp
     int32_t q;               // query row
+    bool lane_rows;          // byte rows fit one lane (dim a multiple of 16, at most 128)
     float qfeat;             // log1p(|q|^2), a stop feature
     const __nv_bfloat16 *mlp_w;  // block shared memory copy of the network (or NULL)
     const float *mlp_b;
@@ -616,6 +621,68 @@ __device__ __forceinline__ void score_chunk(const SearchParams &P, Ctx &C, int32
     }
 }
 
+// Byte rows of at most 128 bytes starting on 16-byte boundaries (dim a multiple of 16): every lane
+// loads the whole row of the neighbour it holds -- eight 16-byte loads in flight per lane -- before
+// the visited marks are resolved, so the gather overlaps the marking atomics and all rows of a chunk
+// arrive in one memory round trip. Rows of neighbours found already visited are dropped unscored and
+// uncounted. Each lane then sums its own row against the query (shared-memory broadcast reads):
+// integer arithmetic, so the value equals dists_bytes' bit for bit.
+__device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, Ctx &C, int32_t e,
+                                                         int log2, int &vis_count, double &dj) {
+    const int v4 = P.dim >> 4;
+    const uint4 *row = reinterpret_cast<const uint4 *>(P.rows8 + int64_t(e < 0 ? 0 : e) * P.dim);
+    uint4 x[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) x[t] = (e >= 0 && t < v4) ? __ldg(row + t) : make_uint4(0u, 0u, 0u, 0u);
+    const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
+    dj = 0.0;
+    if ((um >> C.lane) & 1u) {
+        const uint4 *qv = reinterpret_cast<const uint4 *>(C.q4);
+        uint32_t acc = 0u;
+        if (P.metric == HNSW_B200_L2) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                if (t < v4) {
+                    const uint4 q = qv[t];
+                    uint32_t d = __vabsdiffu4(x[t].x, q.x);
+                    acc = __dp4a(d, d, acc);
+                    d = __vabsdiffu4(x[t].y, q.y);
+                    acc = __dp4a(d, d, acc);
+                    d = __vabsdiffu4(x[t].z, q.z);
+                    acc = __dp4a(d, d, acc);
+                    d = __vabsdiffu4(x[t].w, q.w);
+                    acc = __dp4a(d, d, acc);
+                }
+            }
+            dj = double(acc);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                if (t < v4) {
+                    const uint4 q = qv[t];
+                    acc = __dp4a(x[t].x, q.x, acc);
+                    acc = __dp4a(x[t].y, q.y, acc);
+                    acc = __dp4a(x[t].z, q.z, acc);
+                    acc = __dp4a(x[t].w, q.w, acc);
+                }
+            }
+            dj = -double(acc);
+        }
+    }
+    return um;
+}
+
+// Mark a chunk visited and score its new neighbours (lane j of the returned mask gets dj).
+template <int MODE, bool U8>
+__device__ __forceinline__ uint32_t mark_and_score(const SearchParams &P, Ctx &C, int32_t e, int log2,
+                                                   int &vis_count, double &dj) {
+    if (MODE == MODE_BYTES && HB_LANE_ROWS && C.lane_rows)
+        return mark_score_lane_rows(P, C, e, log2, vis_count, dj);
+    const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
+    score_chunk<MODE, U8>(P, C, e, um, dj);
+    return um;
+}
+
 __device__ __forceinline__ const int32_t *node_links(const SearchParams &P, int32_t c, int layer,
                                                      int &cnt, int &stride) {
     if (layer == 0) {
@@ -824,10 +891,9 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
             if (__shfl_sync(FULL, e, 0) == -2) C.status |= 64;  // consume the load before timing
 #endif
             HB_PROF(2);
-            const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
             HB_PROF(3);
             double dj;
-            score_chunk<MODE, U8>(P, C, e, um, dj);
+            const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
 #ifdef HB_PROFILE
             if (__shfl_sync(FULL, dj, 0) == -12345.0) C.status |= 64;  // consume before timing
 #endif
@@ -1061,9 +1127,8 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? first_link(nb, P.links0_stride, cnt, lane)
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
-            const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
             double dj;
-            score_chunk<MODE, U8>(P, C, e, um, dj);
+            const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
@@ -1177,6 +1242,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
     C.ties = P.ties + slot * P.tie_cap;
     C.spd = FILT ? P.spill_d + slot * P.spill_cap : nullptr;
     C.spi = FILT ? P.spill_i + slot * P.spill_cap : nullptr;
+    C.lane_rows = (P.dim & 15) == 0 && P.dim <= 128;
 
     for (;;) {
         int w = 0;
