@@ -45,7 +45,8 @@ constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;
 constexpr int B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int FILTER_THREADS = 256;
+constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, each taking half of a tile's columns
+constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
 constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s
 
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(tfull + b, 1);
-            mbar_init(tempty + b, 4);
+            mbar_init(tempty + b, EPI_WARPS);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -297,7 +298,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         }
     } else if (warp >= 4) {
         // ---------------------------------------------------------------- epilogue
+        // Warp w reads TMEM lanes 32 (w % 4) .. +31 (its hardware lane quarter: one query per
+        // thread) and columns [half * BN/2, half * BN/2 + BN/2) of each accumulator.
         const int quarter = warp & 3;
+        const int half = (warp - 4) >> 2;
         const int row = quarter * 32 + lane;  // TMEM lane = query row of the tile
         const int q = qt * BM + row;
         const bool qvalid = q < p.nq;
@@ -305,6 +309,8 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         const float thr = qvalid ? p.thr[q] : -INFINITY;
         float *cv = p.cand_val + int64_t(qvalid ? q : 0) * p.cap;
         int32_t *ci = p.cand_id + int64_t(qvalid ? q : 0) * p.cap;
+        const bool l2 = p.metric == HNSW_B200_L2;
+        const bool cosine = p.metric == HNSW_B200_COSINE;
         for (int lt = 0; lt < ntiles; lt++) {
             const int b = lt & 1;
             int ok = 1;
@@ -320,30 +326,39 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int row0 = p.row_begin + (t0 + lt) * BN;
 #pragma unroll 1
-            for (int c = 0; c < BN; c += 32) {
+            for (int c = half * (BN / 2); c < (half + 1) * (BN / 2); c += 32) {
+                const int col0 = row0 + c;
+                // |x|^2 of the 32 columns: the same addresses in every lane (broadcast loads),
+                // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + 32
+                // entries (zero beyond the data rows).
+                float xv[32];
+                if (l2) {
+                    const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const float4 t = __ldg(x4 + i);
+                        xv[4 * i] = t.x;
+                        xv[4 * i + 1] = t.y;
+                        xv[4 * i + 2] = t.z;
+                        xv[4 * i + 3] = t.w;
+                    }
+                }
                 float v[32];
                 tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
-                const int col0 = row0 + c;
+                const int valid = min(32, p.row_end - col0);  // columns that are data rows
                 uint32_t keep = 0;
 #pragma unroll
                 for (int j = 0; j < 32; j++) {
-                    const int id = col0 + j;
-                    float a;
-                    if (p.metric == HNSW_B200_L2)
-                        a = fmaf(-2.f, v[j], qq + __ldg(p.xx + min(id, p.row_end - 1)));
-                    else if (p.metric == HNSW_B200_IP)
-                        a = -v[j];
-                    else
-                        a = 1.f - v[j];
+                    // l2: |q|^2 + |x|^2 - 2 q.x; ip: -q.x; cosine: 1 - q.x (normalised rows)
+                    const float a = l2 ? fmaf(-2.f, v[j], qq + xv[j]) : (cosine ? 1.f - v[j] : -v[j]);
                     v[j] = a;
-                    if (a <= thr && id < p.row_end) keep |= 1u << j;
+                    keep |= (a <= thr && j < valid) ? (1u << j) : 0u;
                 }
                 if (keep && qvalid) {
                     const int cnt = __popc(keep);
-                    const int base = atomicAdd(p.cand_cnt + q, cnt);
-                    int o = base;
+                    int o = atomicAdd(p.cand_cnt + q, cnt);
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
+                    for (int j = 0; j < 32; j++) {  // static indices keep v[] in registers
                         if ((keep >> j) & 1u) {
                             if (o < p.cap) {
                                 cv[o] = v[j];
@@ -382,6 +397,10 @@ __global__ void prep_rows(const T *src, int64_t rows, int dim, int64_t rows_pad,
         __nv_bfloat16 *out = dst + r * kpad;
         if (r >= rows) {
             for (int i = lane; i < kpad; i += 32) out[i] = __float2bfloat16(0.f);
+            if (lane == 0) {
+                norm64[r] = 0.0;
+                sq32[r] = 0.f;
+            }
             continue;
         }
         const T *x = src + r * dim;

@@ -68,6 +68,10 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_SPECULATE
 #define HB_SPECULATE 0
 #endif
+// Layer 0: L2 prefetch of the count and link row of every neighbour that may enter the results.
+#ifndef HB_PREFETCH_LINKS
+#define HB_PREFETCH_LINKS 0
+#endif
 // Byte rows of at most 128 bytes: one lane per neighbour, row loads issued before the visited marks.
 #ifndef HB_LANE_ROWS
 #define HB_LANE_ROWS 1
@@ -909,6 +913,14 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(P.vectors + int64_t(spec_e) * P.dim));
             }
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
+            if (layer == 0 && HB_PREFETCH_LINKS && ((am >> lane) & 1u)) {
+                // Likely future expansions: warm L2 with their count and link row (both lines of a
+                // row that straddles two), so a later pop finds them near.
+                const int32_t *row = P.links0 + int64_t(e) * P.links0_stride;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(row));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(row + P.links0_stride - 1));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(P.count0 + e));
+            }
             while (am) {
                 const int j = __ffs(am) - 1;
                 am &= am - 1;
