@@ -44,6 +44,7 @@ class Graph(ctypes.Structure):
         ("max_level", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
         ("vector_bytes", ctypes.c_void_p),
+        ("node_ids", ctypes.c_void_p),
     ]
 
 

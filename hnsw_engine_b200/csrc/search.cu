@@ -56,7 +56,7 @@ constexpr int WPB = 4;  // warps per block
 #define HB_MINB_EXACT 4
 #endif
 #ifndef HB_MINB_BYTES
-#define HB_MINB_BYTES 6
+#define HB_MINB_BYTES 5
 #endif
 #ifndef HB_NB_EXACT
 #define HB_NB_EXACT 4
@@ -64,13 +64,13 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_NB_BYTES
 #define HB_NB_BYTES 8
 #endif
-// Layer-0 speculation: 0 off, 1 next candidate's links, 2 also L2 prefetch of its neighbours.
-#ifndef HB_SPECULATE
-#define HB_SPECULATE 0
+// Layer 0: admit a chunk's neighbours together (exactly the sequential outcome) instead of one by one.
+#ifndef HB_BATCH_ADMIT
+#define HB_BATCH_ADMIT 1
 #endif
-// Layer 0: L2 prefetch of the count and link row of every neighbour that may enter the results.
-#ifndef HB_PREFETCH_LINKS
-#define HB_PREFETCH_LINKS 0
+// Unfiltered layer 0 visited set: 0 the per-slot bitmap, 1 a per-slot open-addressing hash.
+#ifndef HB_L0_HASH
+#define HB_L0_HASH 0
 #endif
 // Byte rows of at most 128 bytes: one lane per neighbour, row loads issued before the visited marks.
 #ifndef HB_LANE_ROWS
@@ -79,11 +79,11 @@ constexpr int WPB = 4;  // warps per block
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
 #define HB_PROF_DECL unsigned long long hb_t = clock64();
-#define HB_PROF(i)                                              \
-    do {                                                        \
-        unsigned long long hb_n = clock64();                    \
-        if ((threadIdx.x & 31) == 0) atomicAdd(&hb_prof[i], hb_n - hb_t); \
-        hb_t = hb_n;                                            \
+#define HB_PROF(i)                           \
+    do {                                     \
+        unsigned long long hb_n = clock64(); \
+        C.prof[i] += hb_n - hb_t;            \
+        hb_t = hb_n;                         \
     } while (0)
 #else
 #define HB_PROF_DECL
@@ -111,6 +111,7 @@ struct SearchParams {
     const int32_t *links_up;
     const int32_t *count_up;
     int64_t n;
+    const int32_t *node_ids;  // original id of each internal node (NULL: internal = original)
     int32_t dim, links0_stride, links_up_stride, metric;
     int64_t entry_point;
     int32_t max_level;
@@ -170,10 +171,17 @@ constexpr size_t MLP_BYTES = size_t(MLP_BF16) * 2 + size_t(MLP_F32) * 4;
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Result slots per warp: ef_cap entries, plus room for a whole chunk of 32 admissions merged in
+// before the excess is evicted (batched admission), plus one for sequential insertion.
+__host__ __device__ inline int result_slots(int ef_cap) { return ef_cap + 33; }
+
 // Shared memory of one warp: results, query (f64, f32 and bytes), filtered candidates, rerank top-k.
+// two_ids: the graph is stored in an internal node order, so results keep internal ids next to
+// the original ones (otherwise the two are the same array).
 __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filtered, int s_cap,
-                                                  int k_rerank) {
-    size_t b = al16(size_t(ef_cap + 1) * 8) + al16(size_t(ef_cap + 1) * 4) + al16(size_t(dim) * 8) +
+                                                  int k_rerank, bool two_ids) {
+    size_t b = al16(size_t(result_slots(ef_cap)) * 8) +
+               (two_ids ? 2 : 1) * al16(size_t(result_slots(ef_cap)) * 4) + al16(size_t(dim) * 8) +
                al16(size_t(dim) * 4) + al16(size_t(dim));
     if (filtered) b += al16(size_t(s_cap + 1) * 8) + al16(size_t(s_cap + 1) * 4);
     if (k_rerank > 0) b += al16(size_t(k_rerank + 1) * 8) + al16(size_t(k_rerank + 1) * 4);
@@ -183,7 +191,8 @@ __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filt
 struct Ctx {
     int lane;
     double *Rd;
-    int32_t *Ri;
+    int32_t *Ri;  // original id of each result (ordering, output), with the expanded bit
+    int32_t *Rp;  // internal id of each result (memory accesses)
     double *qd;
     float *qf;
     uint32_t *q4;  // query bytes, four per word (byte mode)
@@ -202,13 +211,34 @@ struct Ctx {
     int32_t status;          // uniform across the warp
     int32_t q;               // query row
     bool lane_rows;          // byte rows fit one lane (dim a multiple of 16, at most 128)
+#ifdef HB_PROFILE
+    unsigned long long prof[8];  // cycles per phase of this warp's current query
+#endif
     float qfeat;             // log1p(|q|^2), a stop feature
     const __nv_bfloat16 *mlp_w;  // block shared memory copy of the network (or NULL)
     const float *mlp_b;
 };
 
-__device__ __forceinline__ bool pair_lt(double da, int32_t ia, double db, int32_t ib) {
+// Node arrays may be stored in any order (internal ids, chosen for memory locality); results,
+// and ties between equal distances, use the original ids. Sentinel ids outside [0, n) map to
+// themselves.
+__device__ __forceinline__ int32_t orig_id(const SearchParams &P, int32_t i) {
+#ifdef HB_NO_ID_LOOKUP
+    return i;
+#else
+    return (P.node_ids != nullptr && i >= 0 && i < P.n) ? __ldg(P.node_ids + i) : i;
+#endif
+}
+
+// (distance, id) order of two entries whose ids are comparable as they are.
+__device__ __forceinline__ bool pair_lt_raw(double da, int32_t ia, double db, int32_t ib) {
     return da < db || (da == db && ia < ib);
+}
+
+// (distance, original id) order of two entries given by internal ids.
+__device__ __forceinline__ bool pair_lt(const SearchParams &P, double da, int32_t ia, double db,
+                                        int32_t ib) {
+    return da < db || (da == db && orig_id(P, ia) < orig_id(P, ib));
 }
 
 // ---------------------------------------------------------------------------------------- sorted
@@ -216,7 +246,7 @@ __device__ __forceinline__ bool pair_lt(double da, int32_t ia, double db, int32_
 __device__ __forceinline__ int count_below(const double *Ad, const int32_t *Ai, int m, double d,
                                            int32_t id, int lane) {
     int c = 0;
-    for (int i = lane; i < m; i += 32) c += pair_lt(Ad[i], Ai[i] & ID_MASK, d, id);
+    for (int i = lane; i < m; i += 32) c += pair_lt_raw(Ad[i], Ai[i] & ID_MASK, d, id);
     return __reduce_add_sync(FULL, c);
 }
 
@@ -227,39 +257,42 @@ __device__ __forceinline__ int sorted_rank(const double *Ad, const int32_t *Ai, 
     if (m > 1024) return count_below(Ad, Ai, m, d, id, lane);
     const int step = (m + 31) >> 5;  // entries per chunk
     const int s = lane * step;
-    const bool below = s < m && pair_lt(Ad[s], Ai[s] & ID_MASK, d, id);
+    const bool below = s < m && pair_lt_raw(Ad[s], Ai[s] & ID_MASK, d, id);
     const uint32_t b = __ballot_sync(FULL, below);  // chunks starting below (d, id): a prefix
     const int chunks = __popc(b);
     if (chunks == 0) return 0;
     const int base = (chunks - 1) * step;  // the last chunk starting below holds the boundary
     const int i = base + lane;
-    const bool in = lane < step && i < m && pair_lt(Ad[i], Ai[i] & ID_MASK, d, id);
+    const bool in = lane < step && i < m && pair_lt_raw(Ad[i], Ai[i] & ID_MASK, d, id);
     return base + __popc(__ballot_sync(FULL, in));
 }
 
 // Entries of the descending array [0, m) strictly above (d, id).
-__device__ __forceinline__ int count_above(const double *Ad, const int32_t *Ai, int m, double d,
+__device__ __forceinline__ int count_above(const SearchParams &P, const double *Ad, const int32_t *Ai, int m, double d,
                                            int32_t id, int lane) {
     int c = 0;
-    for (int i = lane; i < m; i += 32) c += pair_lt(d, id, Ad[i], Ai[i]);
+    for (int i = lane; i < m; i += 32) c += pair_lt(P, d, id, Ad[i], Ai[i]);
     return __reduce_add_sync(FULL, c);
 }
 
-// Move [pos, m) to [pos + 1, m + 1), highest chunk first.
-__device__ __forceinline__ void shift_up(double *Ad, int32_t *Ai, int pos, int m, int lane) {
+// Move [pos, m) to [pos + 1, m + 1), highest chunk first (Ap: an optional third array).
+__device__ __forceinline__ void shift_up(double *Ad, int32_t *Ai, int pos, int m, int lane,
+                                         int32_t *Ap = nullptr) {
     for (int top = m - 1; top >= pos; top -= 32) {
         int i = top - lane;
         bool act = i >= pos;
         double d = 0.0;
-        int32_t id = 0;
+        int32_t id = 0, ip = 0;
         if (act) {
             d = Ad[i];
             id = Ai[i];
+            if (Ap) ip = Ap[i];
         }
         __syncwarp();
         if (act) {
             Ad[i + 1] = d;
             Ai[i + 1] = id;
+            if (Ap) Ap[i + 1] = ip;
         }
         __syncwarp();
     }
@@ -810,16 +843,135 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, S
 // ------------------------------------------------------------------------- unfiltered layer search
 // Algorithm 2 with exact reference semantics. On entry R[0] holds the single entry node
 // (unexpanded) and r == 1; on exit R[0..r) is the sorted result list.
+// Admission of one chunk of new neighbours into the sorted results R (unfiltered layer), with the
+// same final R, tie stack and expansion frontier as admitting them one by one in stored order.
+//
+// Sequentially, neighbour j is admitted iff |R| < ef or d_j < W, W the running worst. W is the
+// ef-th smallest distance of R0 (R before the chunk) together with every earlier neighbour of the
+// chunk, admitted or not: a rejected or evicted one is never below the worst that followed. Hence
+//   admitted_j  <=>  #{x in R0 : x.d <= d_j} + #{i < j in the chunk : d_i <= d_j} < ef,
+// which every lane evaluates for its own neighbour at once. Inserting with eviction of the maximum
+// keeps the ef smallest (distance, id) pairs, so the new R is the first ef entries of R0 merged
+// with the admitted set. The evicted entries are the merged tail; the tie stack keeps its entries
+// only if the worst distance did not drop, and gains the unexpanded evicted entries that tie the
+// final worst, pushed in descending (distance, id) order as the evictions would have pushed them.
+// churn (a stop feature) counts admissions that entered the first k at their insertion time.
+__device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32_t e, int32_t eo,
+                                            double dj, uint32_t um, int ef, int &r, double &W,
+                                            int &scan, int &tn, int &churn) {
+    const int lane = C.lane;
+    const int r0 = r;
+    const double W0 = W;
+    const uint32_t cm = __ballot_sync(FULL, ((um >> lane) & 1u) && (r0 < ef || dj < W0));
+    if (!cm) return;
+    const bool inc = (cm >> lane) & 1u;
+    int lo = 0, n_eq = 0, eq_lt = 0;
+    if (inc) {
+        int a = 0, b = r0;  // lo: entries of R0 with distance below dj
+        while (a < b) {
+            const int m = (a + b) >> 1;
+            if (C.Rd[m] < dj) a = m + 1;
+            else b = m;
+        }
+        lo = a;
+        for (int i = a; i < r0 && C.Rd[i] == dj; i++) {  // equal distances: rank by id
+            n_eq++;
+            eq_lt += (C.Ri[i] & ID_MASK) < eo;
+        }
+    }
+    int prev_le = 0;  // earlier candidates of the chunk at or below dj
+    for (uint32_t m = cm; m;) {
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        const double di = __shfl_sync(FULL, dj, i);
+        prev_le += (i < lane && di <= dj);
+    }
+    const bool adm = inc && lo + n_eq + prev_le < ef;
+    const uint32_t A = __ballot_sync(FULL, adm);
+    if (!A) return;
+    int rank_a = 0, rank_prev = 0;  // admitted pairs below mine: all of them, and earlier ones
+    for (uint32_t m = A; m;) {
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        const double di = __shfl_sync(FULL, dj, i);
+        const int32_t ii = __shfl_sync(FULL, eo, i);
+        const bool lt = di < dj || (di == dj && ii < eo);
+        rank_a += lt;
+        rank_prev += (lt && i < lane);
+    }
+    const int pos_r0 = lo + eq_lt;  // entries of R0 below (dj, e)
+    const int fpos = pos_r0 + rank_a;
+    churn += __popc(__ballot_sync(FULL, adm && pos_r0 + rank_prev < P.k));
+    const int pmin = __reduce_min_sync(FULL, adm ? pos_r0 : 0x7fffffff);
+    const int fmin = __reduce_min_sync(FULL, adm ? fpos : 0x7fffffff);
+    // Move R0[p] (p >= pmin) up by the admitted entries that precede it, highest chunk first.
+    for (int top = r0 - 1; top >= pmin; top -= 32) {
+        const int p = top - lane;
+        const bool act = p >= pmin;
+        double d = 0.0;
+        int32_t id = 0, ip = 0;
+        int sft = 0;
+        if (act) {
+            d = C.Rd[p];
+            id = C.Ri[p];
+            ip = C.Rp[p];
+        }
+        for (uint32_t m = A; m;) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1;
+            sft += __shfl_sync(FULL, pos_r0, i) <= p;
+        }
+        __syncwarp();
+        if (act) {
+            C.Rd[p + sft] = d;
+            C.Ri[p + sft] = id;
+            C.Rp[p + sft] = ip;
+        }
+        __syncwarp();
+    }
+    if (adm) {
+        C.Rd[fpos] = dj;
+        C.Ri[fpos] = eo;
+        C.Rp[fpos] = e;
+    }
+    __syncwarp();
+    int rn = r0 + __popc(A);
+    if (rn > ef) {
+        const int nev = rn - ef;  // at most 32
+        const double wf = C.Rd[ef - 1];
+        if (r0 == ef && wf != W0) tn = 0;  // the worst dropped: earlier ties are too far now
+        bool push = false;
+        int32_t pid = 0;
+        if (lane < nev) {
+            pid = C.Rp[ef + lane] & ID_MASK;
+            push = C.Rd[ef + lane] == wf && !(C.Ri[ef + lane] & EXP_BIT);
+        }
+        const uint32_t pm = __ballot_sync(FULL, push);
+        const int idx = tn + __popc(pm >> lane) - 1;  // the largest pair was evicted (pushed) first
+        if (push && idx < P.tie_cap) C.ties[idx] = pid;
+        tn += __popc(pm);
+        if (tn > P.tie_cap) {
+            C.status |= ST_TIES;
+            tn = P.tie_cap;
+        }
+        rn = ef;
+    }
+    __syncwarp();
+    r = rn;
+    W = C.Rd[r - 1];
+    scan = min(scan, fmin);
+}
+
 template <int MODE, bool U8>
 __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, int log2, int &r) {
     const int lane = C.lane;
-    if (layer > 0) {
+    if (layer > 0 || (HB_L0_HASH && log2 > 0)) {
         vis_clear(C.vis, log2, lane);
-        if (lane == 0) vis_insert(C.vis, log2, C.Ri[0] & ID_MASK);
+        if (lane == 0) vis_insert(C.vis, log2, C.Rp[0] & ID_MASK);
         __syncwarp();
     } else {
         log2 = 0;  // bitmap
-        bitmap_begin(P, C, C.Ri[0] & ID_MASK);
+        bitmap_begin(P, C, C.Rp[0] & ID_MASK);
     }
     int vis_count = 1;
     const int vis_lim = log2 > 0 ? ((1 << log2) >> 2) * 3 : 0x7fffffff;
@@ -827,9 +979,6 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
     int scan = 0;  // every result before `scan` is expanded
     int tn = 0;    // tie stack depth
     const bool track = layer == 0 && (P.trace_feat != nullptr || C.mlp_w != nullptr);
-    // Speculation (layer 0): the links of the next unexpanded result are loaded while the current
-    // node is processed; they are used if that node is indeed popped next.
-    int32_t spec_c = -1, spec_cnt = 0, spec_e = -1;
     StopState S{0, 0, 0, 0, 0.f, 0.f, log1pf(float(C.Rd[0]))};
     HB_PROF_DECL
     for (;;) {
@@ -841,10 +990,11 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
             const uint32_t b = __ballot_sync(FULL, un);
             if (b) {
                 const int p = scan + __ffs(b) - 1;
-                c = C.Ri[p];
+                c = C.Rp[p] & ID_MASK;
+                const int32_t co = C.Ri[p];
                 scan = p + 1;
                 __syncwarp();
-                if (lane == 0) C.Ri[p] = c | EXP_BIT;
+                if (lane == 0) C.Ri[p] = co | EXP_BIT;
                 __syncwarp();
                 break;
             }
@@ -853,43 +1003,16 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
         if (c < 0) {
             if (tn == 0) break;
             tn--;
-            c = C.ties[tn];  // ties W: expanded after every result (they compare greater)
+            c = C.ties[tn];  // ties W (internal ids): expanded after every result
         }
         C.nhops++;
         HB_PROF(1);
         int cnt, stride;
-        const int32_t *nb;
-        int32_t e0;
-        if (c == spec_c) {  // loaded during the previous expansion
-            cnt = spec_cnt;
-            stride = P.links0_stride;
-            nb = P.links0 + int64_t(c) * P.links0_stride;
-            e0 = lane < cnt ? spec_e : -1;
-        } else {
-            nb = node_links(P, c, layer, cnt, stride);
-            e0 = first_link(nb, stride, cnt, lane);
-        }
-        if (layer == 0 && HB_SPECULATE) {
-            // Next guess: the first unexpanded result after the popped one (the tie stack's top if
-            // none); its count and first link chunk are loaded now, concurrently with this node.
-            int32_t c2 = -1;
-            for (int b0 = scan; b0 < r; b0 += 32) {
-                const int i = b0 + lane;
-                const uint32_t m = __ballot_sync(FULL, i < r && !(C.Ri[i] & EXP_BIT));
-                if (m) {
-                    c2 = C.Ri[b0 + __ffs(m) - 1];
-                    break;
-                }
-            }
-            if (c2 < 0 && tn > 0) c2 = C.ties[tn - 1];
-            spec_c = c2;
-            if (c2 >= 0) {
-                spec_cnt = __ldg(P.count0 + c2);
-                spec_e = lane < P.links0_stride ? __ldg(P.links0 + int64_t(c2) * P.links0_stride + lane) : -1;
-            }
-        }
+        const int32_t *nb = node_links(P, c, layer, cnt, stride);
+        const int32_t e0 = first_link(nb, stride, cnt, lane);
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? e0 : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
+            const int32_t eo = e >= 0 ? orig_id(P, e) : -1;  // needed only at admission
 #ifdef HB_PROFILE
             __syncwarp();
             if (__shfl_sync(FULL, e, 0) == -2) C.status |= 64;  // consume the load before timing
@@ -903,35 +1026,25 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
 #endif
             HB_PROF(5);
             C.ndist += __popc(um);
-            if (layer == 0 && HB_SPECULATE >= 2 && base == 0 && spec_c >= 0 && lane < spec_cnt &&
-                spec_e >= 0) {
-                // Warm L2 with the guessed node's neighbours: their bitmap words and rows.
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(C.vbits + (spec_e >> 5)));
-                if (MODE == MODE_BYTES)
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(P.rows8 + int64_t(spec_e) * P.dim));
-                else if (!U8)
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(P.vectors + int64_t(spec_e) * P.dim));
+            if (layer == 0 && HB_BATCH_ADMIT) {
+                admit_chunk(P, C, e, eo, dj, um, ef, r, W, scan, tn, S.churn);
+                HB_PROF(4);
+                continue;
             }
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
-            if (layer == 0 && HB_PREFETCH_LINKS && ((am >> lane) & 1u)) {
-                // Likely future expansions: warm L2 with their count and link row (both lines of a
-                // row that straddles two), so a later pop finds them near.
-                const int32_t *row = P.links0 + int64_t(e) * P.links0_stride;
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(row));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(row + P.links0_stride - 1));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(P.count0 + e));
-            }
             while (am) {
                 const int j = __ffs(am) - 1;
                 am &= am - 1;
                 const double d = __shfl_sync(FULL, dj, j);
-                const int32_t id = __shfl_sync(FULL, e, j);
+                const int32_t id = __shfl_sync(FULL, eo, j);
+                const int32_t pid = __shfl_sync(FULL, e, j);
                 if (!(r < ef || d < W)) continue;  // uniform
                 const int pos = sorted_rank(C.Rd, C.Ri, r, d, id, lane);
-                shift_up(C.Rd, C.Ri, pos, r, lane);
+                shift_up(C.Rd, C.Ri, pos, r, lane, C.Rp != C.Ri ? C.Rp : nullptr);
                 if (lane == 0) {
                     C.Rd[pos] = d;
                     C.Ri[pos] = id;
+                    C.Rp[pos] = pid;
                 }
                 __syncwarp();
                 r++;
@@ -944,7 +1057,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
                     if (ed == C.Rd[ef - 1]) {
                         if (!(ei & EXP_BIT)) {  // still a candidate, tied with the worst
                             if (tn < P.tie_cap) {
-                                if (lane == 0) C.ties[tn] = ei;
+                                if (lane == 0) C.ties[tn] = C.Rp[ef] & ID_MASK;
                                 tn++;
                             } else {
                                 C.status |= ST_TIES;
@@ -962,6 +1075,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
         if (vis_count > vis_lim) C.status |= ST_VISITED;
         if (C.status) break;
         if (track && (++S.hops0 % STOP_EVERY) == 0 && stop_checkpoint(P, C, S, r, scan, W)) break;
+        HB_PROF(6);
         __syncwarp();
     }
     if (track && P.trace_feat && lane == 0) {
@@ -993,11 +1107,11 @@ __device__ __forceinline__ void spill_push(const SearchParams &P, Ctx &C, Cands 
 
 __device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &K, double d,
                                           int32_t id) {
-    if (K.g > 0 && !pair_lt(d, id, K.gd, K.gi)) {  // not below the spill minimum
+    if (K.g > 0 && !pair_lt(P, d, id, K.gd, K.gi)) {  // not below the spill minimum
         spill_push(P, C, K, d, id);
         return;
     }
-    const int pos = count_above(C.Sd, C.Si, K.s, d, id, C.lane);
+    const int pos = count_above(P, C.Sd, C.Si, K.s, d, id, C.lane);
     shift_up(C.Sd, C.Si, pos, K.s, C.lane);
     if (C.lane == 0) {
         C.Sd[pos] = d;
@@ -1032,14 +1146,14 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
             id = C.spi[i];
             if (prune && d > Wp) v = false;
         }
-        uint32_t cm = __ballot_sync(FULL, v && (s < B || pair_lt(d, id, C.Sd[0], C.Si[0])));
+        uint32_t cm = __ballot_sync(FULL, v && (s < B || pair_lt(P, d, id, C.Sd[0], C.Si[0])));
         while (cm) {
             const int j = __ffs(cm) - 1;
             cm &= cm - 1;
             const double xd = __shfl_sync(FULL, d, j);
             const int32_t xi = __shfl_sync(FULL, id, j);
-            if (!(s < B || pair_lt(xd, xi, C.Sd[0], C.Si[0]))) continue;
-            const int pos = count_above(C.Sd, C.Si, s, xd, xi, lane);
+            if (!(s < B || pair_lt(P, xd, xi, C.Sd[0], C.Si[0]))) continue;
+            const int pos = count_above(P, C.Sd, C.Si, s, xd, xi, lane);
             shift_up(C.Sd, C.Si, pos, s, lane);
             if (lane == 0) {
                 C.Sd[pos] = xd;
@@ -1051,7 +1165,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
                 shift_down(C.Sd, C.Si, 0, s, lane);
                 s--;
             }
-            if (s == B) cm &= __ballot_sync(FULL, pair_lt(d, id, C.Sd[0], C.Si[0]));
+            if (s == B) cm &= __ballot_sync(FULL, pair_lt(P, d, id, C.Sd[0], C.Si[0]));
         }
     }
     // Compact the spill: keep entries not selected (above S's maximum) and not pruned.
@@ -1068,7 +1182,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
         if (i < K.g) {
             d = C.spd[i];
             id = C.spi[i];
-            keep = !(prune && d > Wp) && pair_lt(td, ti, d, id);
+            keep = !(prune && d > Wp) && pair_lt(P, td, ti, d, id);
         }
         const uint32_t km = __ballot_sync(FULL, keep);
         __syncwarp();
@@ -1076,7 +1190,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
             const int o = w + __popc(km & ((1u << lane) - 1u));
             C.spd[o] = d;
             C.spi[o] = id;
-            if (pair_lt(d, id, md, mi)) {
+            if (pair_lt(P, d, id, md, mi)) {
                 md = d;
                 mi = id;
             }
@@ -1088,7 +1202,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
     for (int o = 16; o > 0; o >>= 1) {
         const double od = __shfl_xor_sync(FULL, md, o);
         const int32_t oi = __shfl_xor_sync(FULL, mi, o);
-        if (pair_lt(od, oi, md, mi)) {
+        if (pair_lt(P, od, oi, md, mi)) {
             md = od;
             mi = oi;
         }
@@ -1105,16 +1219,17 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
 // closest candidate is strictly farther than the worst.
 template <int MODE, bool U8>
 __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2, double d0,
-                                int32_t e0, int &r) {
+                                int32_t e0, int32_t o0, int &r) {
     const int lane = C.lane;
     log2 = 0;  // bitmap
     bitmap_begin(P, C, e0);
-    if (lane == 0) {
+    if (lane == 0) {  // candidates hold internal ids; results hold both
         C.Sd[0] = d0;
         C.Si[0] = e0;
         if (is_allowed(P.allowed, e0)) {
             C.Rd[0] = d0;
-            C.Ri[0] = e0;
+            C.Ri[0] = o0;
+            C.Rp[0] = e0;
         }
     }
     __syncwarp();
@@ -1139,6 +1254,7 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? first_link(nb, P.links0_stride, cnt, lane)
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
+            const int32_t eo = e >= 0 ? orig_id(P, e) : -1;
             double dj;
             const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);
@@ -1151,11 +1267,13 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
                 if (!(r < ef || d < W)) continue;
                 cand_push(P, C, K, d, id);
                 if (is_allowed(P.allowed, id)) {
-                    const int pos = count_below(C.Rd, C.Ri, r, d, id, lane);
-                    shift_up(C.Rd, C.Ri, pos, r, lane);
+                    const int32_t ido = __shfl_sync(FULL, eo, j);  // uniform branch
+                    const int pos = count_below(C.Rd, C.Ri, r, d, ido, lane);
+                    shift_up(C.Rd, C.Ri, pos, r, lane, C.Rp != C.Ri ? C.Rp : nullptr);
                     if (lane == 0) {
                         C.Rd[pos] = d;
-                        C.Ri[pos] = id;
+                        C.Ri[pos] = ido;
+                        C.Rp[pos] = id;
                     }
                     __syncwarp();
                     r++;
@@ -1181,15 +1299,15 @@ __device__ int rerank_epilogue(const SearchParams &P, Ctx &C, int m) {
     for (int base = 0; base < m; base += 32) {
         const int i = base + lane;
         const bool has = i < m;
-        const int32_t id = has ? (C.Ri[i] & ID_MASK) : -1;
-        const double d = has ? dist_seq_f64<false>(P, id, C.qd) : INFINITY;
+        const int32_t id = has ? (C.Ri[i] & ID_MASK) : -1;  // original id
+        const double d = has ? dist_seq_f64<false>(P, C.Rp[i] & ID_MASK, C.qd) : INFINITY;
         uint32_t am = __ballot_sync(FULL, has);
         while (am) {
             const int j = __ffs(am) - 1;
             am &= am - 1;
             const double xd = __shfl_sync(FULL, d, j);
             const int32_t xi = __shfl_sync(FULL, id, j);
-            if (a == k && !pair_lt(xd, xi, C.Ad[k - 1], C.Ai[k - 1])) continue;
+            if (a == k && !pair_lt_raw(xd, xi, C.Ad[k - 1], C.Ai[k - 1])) continue;
             const int pos = count_below(C.Ad, C.Ai, a, xd, xi, lane);
             shift_up(C.Ad, C.Ai, pos, a, lane);
             if (lane == 0) {
@@ -1210,14 +1328,20 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const bool rerank = P.rerank_queries != nullptr;
-    const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0);
+    const bool two_ids = P.node_ids != nullptr;
+    const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids);
     unsigned char *p = smem + size_t(warp) * wb;
     Ctx C;
     C.lane = lane;
     C.Rd = reinterpret_cast<double *>(p);
-    p += al16(size_t(P.ef_cap + 1) * 8);
+    p += al16(size_t(result_slots(P.ef_cap)) * 8);
     C.Ri = reinterpret_cast<int32_t *>(p);
-    p += al16(size_t(P.ef_cap + 1) * 4);
+    p += al16(size_t(result_slots(P.ef_cap)) * 4);
+    C.Rp = C.Ri;  // same ids: one array (reads of Rp mask the expanded bit)
+    if (two_ids) {
+        C.Rp = reinterpret_cast<int32_t *>(p);
+        p += al16(size_t(result_slots(P.ef_cap)) * 4);
+    }
     C.qd = reinterpret_cast<double *>(p);
     p += al16(size_t(P.dim) * 8);
     C.qf = reinterpret_cast<float *>(p);
@@ -1284,6 +1408,9 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
         C.nhops = 0;
         C.status = 0;
         C.q = q;
+#ifdef HB_PROFILE
+        for (int i = 0; i < 8; i++) C.prof[i] = 0;
+#endif
         if (!FILT && (P.stop_mlp || P.trace_feat)) {
             double ss = 0.0;
             for (int i = lane; i < dim; i += 32) ss += C.qd[i] * C.qd[i];
@@ -1292,30 +1419,34 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
             C.qfeat = log1pf(float(ss));
         }
         // Entry point, then greedy descent (ef = 1) through the upper layers.
-        int32_t e0 = int32_t(P.entry_point);
+        int32_t e0 = int32_t(P.entry_point);  // internal id
+        int32_t o0 = orig_id(P, e0);            // original id
         double d0 = dist_one<MODE, U8>(P, C, e0);
         C.ndist++;
         int r = 1;
         for (int layer = P.max_level; layer > 0 && !C.status; layer--) {
             if (lane == 0) {
                 C.Rd[0] = d0;
-                C.Ri[0] = e0;
+                C.Ri[0] = o0;
+                C.Rp[0] = e0;
             }
             __syncwarp();
             r = 1;
             layer_search<MODE, U8>(P, C, layer, 1, P.vis_up_log2, r);
             d0 = C.Rd[0];
-            e0 = C.Ri[0] & ID_MASK;
+            o0 = C.Ri[0] & ID_MASK;
+            e0 = C.Rp[0] & ID_MASK;
             __syncwarp();
         }
         const int ef0 = max(__ldg(P.ef + q), P.k_search);
         if (!C.status) {
             if (FILT) {
-                layer0_filtered<MODE, U8>(P, C, ef0, P.vis_log2, d0, e0, r);
+                layer0_filtered<MODE, U8>(P, C, ef0, P.vis_log2, d0, e0, o0, r);
             } else {
                 if (lane == 0) {
                     C.Rd[0] = d0;
-                    C.Ri[0] = e0;
+                    C.Ri[0] = o0;
+                    C.Rp[0] = e0;
                 }
                 __syncwarp();
                 r = 1;
@@ -1349,6 +1480,10 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
                 od[i] = i < r ? C.Rd[i] : INFINITY;
             }
         }
+#ifdef HB_PROFILE
+        if (lane == 0)
+            for (int i = 0; i < 8; i++) atomicAdd(&hb_prof[i], C.prof[i]);
+#endif
         if (lane == 0) {
             P.status[q] = 0;
             if (P.out_ctr) {
@@ -1590,7 +1725,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
     const int s_cap = 256;
-    const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr);
+    const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr, g.node_ids != nullptr);
     const bool use_mlp = a->stop_mlp != nullptr && !filt;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (a->trace_feat && (!a->trace_dk || !a->trace_count || !a->trace_hops || a->trace_cap < 1))
@@ -1631,6 +1766,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.links_up = g.links_up;
     P.count_up = g.count_up;
     P.n = g.n;
+    P.node_ids = g.node_ids;
     P.dim = g.dim;
     P.links0_stride = g.links0_stride;
     P.links_up_stride = g.links_up_stride;
@@ -1666,7 +1802,9 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     for (int attempt = 0; attempt < 6; attempt++) {
         const int blocks = int(std::min<int64_t>(int64_t(h.sms) * bps, (n_work + WPB - 1) / WPB));
         const int64_t slots = int64_t(blocks) * WPB;
-        const int64_t vis_stride = int64_t(1) << vis_up_log2;  // layer 0 uses the bitmap
+        // Unfiltered layer 0 uses the bitmap unless built with its hash (HB_L0_HASH).
+        const int64_t vis_stride = int64_t(1) << (HB_L0_HASH && !filt ? std::max(vis_log2, vis_up_log2)
+                                                                      : vis_up_log2);
         if (int rc = h.vis.ensure(size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
         if (h.bits_dirty && h.vbits.ptr) {
             CUDA_TRY(cudaMemsetAsync(h.vbits.ptr, 0, h.vbits.bytes, s));
@@ -1803,7 +1941,7 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
                          : (a->dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64);
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
-    const size_t wb = warp_smem_bytes(ef_cap, g.dim, false, 256, krr);
+    const size_t wb = warp_smem_bytes(ef_cap, g.dim, false, 256, krr, g.node_ids != nullptr);
     const bool use_mlp = a->stop_mlp != nullptr;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (smem_block > 227 * 1024) return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory");
@@ -1861,6 +1999,7 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     P.links_up = g.links_up;
     P.count_up = g.count_up;
     P.n = g.n;
+    P.node_ids = g.node_ids;
     P.dim = g.dim;
     P.links0_stride = g.links0_stride;
     P.links_up_stride = g.links_up_stride;

@@ -24,6 +24,10 @@ from numpy.typing import NDArray
 from . import _lib
 
 EXACT_LIMIT = float(2**24)
+# Graphs of at least this many nodes with byte rows are stored on the GPU in a locality order (see
+# DeviceGraph._build_internal_order); smaller ones fit in L2 and keep the reference's order.
+LOCALITY_MIN_NODES = 65536
+LOCALITY_CELLS = 256
 
 
 def _dev_ptr(t: torch.Tensor | None) -> int | None:
@@ -61,6 +65,7 @@ class DeviceGraph:
         max_level: int,
         metric: str,
         device: str | torch.device = "cuda",
+        locality: bool | None = None,
     ) -> None:
         self.lib = _lib.load()
         self.device = torch.device(device)
@@ -101,10 +106,84 @@ class DeviceGraph:
                 and self._hi.max() <= 255):
             with torch.cuda.device(self.device):
                 self.vector_bytes = to_device(host_vectors.astype(np.uint8), torch.uint8, self.device)
+        # Automatic: large graphs searched by the byte kernel, whose gathers are the bottleneck (the
+        # float64 kernel is bound by its arithmetic and gains nothing from the order).
+        if locality is None:
+            locality = self.n >= LOCALITY_MIN_NODES and self.vector_bytes is not None
+        self.locality = bool(locality) and self.n > 1
+        self.order: torch.Tensor | None = None  # internal node -> original id (None: identity)
+        self._order_host: NDArray[np.int64] | None = None
+        self._internal: dict[str, Any] = {}
+        if self.locality:
+            self._build_internal_order()
         self._handle = ctypes.c_void_p()
         self._open()
 
+    # ------------------------------------------------------------------------ node order
+    def _build_internal_order(self) -> None:
+        """Store the graph in cell order: nodes grouped by their nearest of 256 sampled pivot rows
+        (ties to the lower original id), so that a search's visited nodes, rows and link rows fall
+        in a few contiguous ranges. The library reads every array in this internal order and maps
+        back to original ids for results and for ties between equal distances, so results are the
+        reference's exactly; only memory locality changes."""
+        from .exact_knn import exact_search
+
+        dev = self.device
+        n = self.n
+        cells = min(LOCALITY_CELLS, n)
+        pick = np.sort(np.random.default_rng(0).choice(n, cells, replace=False))
+        with torch.cuda.device(dev):
+            pivots = self.vectors[torch.from_numpy(pick).to(dev)].contiguous()
+            nearest, _ = exact_search(pivots, self.vectors, 1, "l2")
+            order = torch.sort(nearest[:, 0], stable=True).indices  # internal -> original
+            new_of_old = torch.empty_like(order)
+            new_of_old[order] = torch.arange(n, device=dev)
+
+            def relink(links: torch.Tensor, counts: torch.Tensor) -> torch.Tensor:
+                valid = torch.arange(links.shape[1], device=dev)[None, :] < counts[:, None]
+                mapped = new_of_old[links.clamp(0, n - 1).long()].to(torch.int32)
+                return torch.where(valid, mapped, links).contiguous()
+
+            inner = self._internal
+            inner["vectors"] = self.vectors[order].contiguous()
+            inner["vector_bytes"] = (self.vector_bytes[order].contiguous()
+                                     if self.vector_bytes is not None else None)
+            inner["count0"] = self.count0[order].contiguous()
+            inner["links0"] = relink(self.links0[order], inner["count0"])
+            inner["upper_offset"] = self.upper_offset[order].contiguous()
+            inner["links_up"] = relink(self.links_up, self.count_up)
+            inner["entry_point"] = int(new_of_old[self.entry_point].item())
+            inner["node_ids"] = order.to(torch.int32).contiguous()
+        self.order = order
+        self._order_host = order.cpu().numpy()
+
+    def internal_mask(self, mask: NDArray[np.bool_]) -> NDArray[np.bool_]:
+        """A filter mask over original ids, rearranged into the internal node order."""
+        return mask if self._order_host is None else np.ascontiguousarray(mask[self._order_host])
+
     def _graph_struct(self) -> _lib.Graph:
+        inner = self._internal
+        if inner:
+            return _lib.Graph(
+                vectors=_dev_ptr(inner["vectors"]),
+                codes=_dev_ptr(inner.get("codes")),
+                links0=_dev_ptr(inner["links0"]),
+                count0=_dev_ptr(inner["count0"]),
+                upper_offset=_dev_ptr(inner["upper_offset"]),
+                links_up=_dev_ptr(inner["links_up"]),
+                count_up=_dev_ptr(self.count_up),
+                n=self.n,
+                rows=self.rows,
+                dim=self.dim,
+                links0_stride=self.links0_stride,
+                links_up_stride=self.links_up_stride,
+                metric=_lib.METRIC_CODES[self.metric],
+                entry_point=inner["entry_point"],
+                max_level=self.max_level,
+                reserved=0,
+                vector_bytes=_dev_ptr(inner["vector_bytes"]),
+                node_ids=_dev_ptr(inner["node_ids"]),
+            )
         return _lib.Graph(
             vectors=_dev_ptr(self.vectors),
             codes=_dev_ptr(self.codes),
@@ -123,6 +202,7 @@ class DeviceGraph:
             max_level=self.max_level,
             reserved=0,
             vector_bytes=_dev_ptr(self.vector_bytes),
+            node_ids=None,
         )
 
     def _open(self) -> None:
@@ -139,6 +219,8 @@ class DeviceGraph:
             raise ValueError(f"codes must be uint8 with shape {(self.n, self.dim)}")
         with torch.cuda.device(self.device):
             self.codes = to_device(codes, torch.uint8, self.device)
+            if self._internal:
+                self._internal["codes"] = self.codes[self.order].contiguous()
         self._open()
 
     def close(self) -> None:
@@ -188,6 +270,34 @@ class DeviceGraph:
             bound = (np.abs(q) * np.maximum(np.abs(lo), np.abs(hi))).sum(axis=1).max()
         return bool(bound < EXACT_LIMIT)
 
+    def choose_mode_device(self, q: torch.Tensor, codes: bool) -> int:
+        """:meth:`choose_mode` for queries already on this GPU: the same rules, evaluated by a few
+        device reductions and one small copy back, instead of a host pass over the batch."""
+        if q.numel() == 0:
+            return _lib.DIST_F64
+        qd = q.to(torch.float64)
+        st = torch.stack([(qd != torch.round(qd)).any().to(torch.float64), qd.min(), qd.max()]).cpu()
+        integer = not bool(st[0])
+        if self.metric == "cosine" or not integer:
+            return _lib.DIST_F64
+        rows_ok = codes or self.vector_bytes is not None
+        if self.dim % 4 == 0 and rows_ok and float(st[1]) >= 0 and float(st[2]) <= 255:
+            return _lib.DIST_BYTES
+        if codes:
+            lo, hi = np.zeros(self.dim), np.full(self.dim, 255.0)
+        elif self._integer:
+            lo, hi = self._lo, self._hi
+        else:
+            return _lib.DIST_F64
+        lo_t = torch.from_numpy(np.asarray(lo, dtype=np.float64)).to(qd.device)
+        hi_t = torch.from_numpy(np.asarray(hi, dtype=np.float64)).to(qd.device)
+        if self.metric == "l2":
+            span = torch.maximum((qd - lo_t).abs(), (hi_t - qd).abs())
+            bound = (span * span).sum(dim=1).max()
+        else:
+            bound = (qd.abs() * torch.maximum(lo_t.abs(), hi_t.abs())).sum(dim=1).max()
+        return _lib.DIST_EXACT_F32 if float(bound) < EXACT_LIMIT else _lib.DIST_F64
+
     # ------------------------------------------------------------------------------ search
     def search(
         self,
@@ -210,7 +320,8 @@ class DeviceGraph:
 
         ``queries``: (nq, dim) float32 prepared queries, or float64 code-space queries with
         ``use_codes``. ``ef``: scalar or (nq,) raw efSearch (layer 0 uses ``max(ef, k_search)``).
-        ``allowed``: bool mask (n,) or a device uint32 bitmap. ``rerank_queries``: float32 prepared
+        ``allowed``: bool mask (n,) over original ids, or a device uint32 bitmap over internal
+        ids (``pack_mask(internal_mask(mask))``). ``rerank_queries``: float32 prepared
         queries for the fused exact re-rank of the first ``k_search`` beam entries. ``stop``:
         ``(packed network, threshold)`` for the learned early termination; ``trace``: device
         buffers ``(features (nq, cap, 12) f32, first 16 result distances (nq, cap, 16) f64,
@@ -221,11 +332,10 @@ class DeviceGraph:
         nq = int(queries.shape[0])
         ks = int(k if k_search is None else k_search)
         q_f64 = use_codes
-        if dist_mode is None:
-            host_q = queries.detach().cpu().numpy() if isinstance(queries, torch.Tensor) else queries
-            dist_mode = self.choose_mode(host_q, use_codes)
         with torch.cuda.device(dev):
             q = to_device(queries, torch.float64 if q_f64 else torch.float32, dev)
+            if dist_mode is None:
+                dist_mode = self.choose_mode_device(q, use_codes)
             if isinstance(ef, torch.Tensor):
                 ef_t = ef.to(device=dev, dtype=torch.int32).contiguous()
                 ef_max = int(ef_t.max().item()) if nq else 1
@@ -242,7 +352,7 @@ class DeviceGraph:
                 else:
                     mask = np.asarray(allowed.cpu() if isinstance(allowed, torch.Tensor) else allowed)
                     frac = float(mask.mean()) if mask.size else 1.0
-                    bitmap = to_device(pack_mask(mask).view(np.int32), torch.int32, dev)
+                    bitmap = to_device(pack_mask(self.internal_mask(mask)).view(np.int32), torch.int32, dev)
             rq = None
             if rerank_queries is not None:
                 rq = to_device(rerank_queries, torch.float32, dev)

@@ -106,7 +106,9 @@ class HNSWIndex:
 
     Open one with :meth:`load_native` (a ``save_native`` directory) or :meth:`from_arrays`.
     Constructor parameters mirror the reference's (``index.py:115-149``); only ``ef_search`` and
-    ``metric`` affect searching.
+    ``metric`` affect searching. Extensions: ``device``, and ``locality`` (store the graph on the
+    GPU in a cell order for memory locality; ``None`` turns it on from 65,536 nodes when the vectors
+    are integers in [0, 255]; results are the same either way).
     """
 
     def __init__(
@@ -123,6 +125,7 @@ class HNSWIndex:
         m_L: float | None = None,
         engine: str = "b200",
         device: str | torch.device = "cuda",
+        locality: bool | None = None,
     ) -> None:
         self._dim = check_int(dim, "dim", minimum=1)
         self._metric = validate_metric(metric)
@@ -138,6 +141,7 @@ class HNSWIndex:
         self._m_L = 1.0 / math.log(self._M) if m_L is None else float(m_L)
         self._engine_name = engine
         self._device = device
+        self._locality = locality  # device node order: None = automatic (see engine.DeviceGraph)
         self._graph: DeviceGraph | None = None
         self._arrays: dict[str, NDArray[Any]] | None = None
         self._size = 0
@@ -148,12 +152,12 @@ class HNSWIndex:
     @classmethod
     def load_native(
         cls, directory: str | Path, mmap: bool = True, validate: bool = True,
-        device: str | torch.device = "cuda",
+        device: str | torch.device = "cuda", locality: bool | None = None,
     ) -> HNSWIndex:
         """Open a directory written by the reference's ``HNSWIndex.save_native``."""
         meta, arrays = read_native(directory, mmap=mmap)
         params = {k: v for k, v in meta["params"].items() if k != "engine"}
-        index = cls(**params, device=device)
+        index = cls(**params, device=device, locality=locality)
         index._meta_extra = {"rng_state": meta.get("rng_state")}
         index._attach(arrays, int(meta["entry_point"]), int(meta["max_level"]), validate)
         return index
@@ -178,7 +182,8 @@ class HNSWIndex:
         self._entry_point = entry_point
         self._max_level = max_level
         if self._size:
-            self._graph = DeviceGraph(self._arrays, entry_point, max_level, self._metric, self._device)
+            self._graph = DeviceGraph(self._arrays, entry_point, max_level, self._metric, self._device,
+                                      locality=self._locality)
 
     # ---------------------------------------------------------------------- properties
     @property

@@ -62,6 +62,13 @@ typedef struct hnsw_b200_graph {
     int32_t reserved;
     const uint8_t *vector_bytes; /* (n, dim) uint8 copy of integer-valued vectors in [0, 255] (the
                                     same values, one byte each), or NULL; enables the byte mode */
+    const int32_t *node_ids;     /* NULL: the arrays are in the reference's node order. Otherwise
+                                    the arrays are stored in an internal node order chosen for
+                                    memory locality: row i of every per-node array belongs to the
+                                    node whose original id is node_ids[i], link entries and
+                                    entry_point are internal ids, and the allowed bitmap is indexed
+                                    by internal id. Results are original ids, and equal distances
+                                    order by original id, so results equal the reference's. */
 } hnsw_b200_graph_t;
 
 /* Distance arithmetic of one search call. */

@@ -15,19 +15,23 @@ from conftest import QUANT_CASES, SEARCH_CASES, case_arrays, iter_search_runs, l
 pytestmark = pytest.mark.gpu
 
 
-def _index(arrays, ep, ml, metric, M):
+def _index(arrays, ep, ml, metric, M, locality=None):
     from hnsw_engine_b200 import HNSWIndex
 
-    return HNSWIndex.from_arrays(arrays, ep, ml, dim=arrays["vectors"].shape[1], metric=metric, M=M)
+    return HNSWIndex.from_arrays(arrays, ep, ml, dim=arrays["vectors"].shape[1], metric=metric, M=M,
+                                 locality=locality)
 
 
+@pytest.mark.parametrize("locality", [False, True], ids=["reference_order", "cell_order"])
 @pytest.mark.parametrize("name", SEARCH_CASES)
-def test_search_matches_reference_bit_for_bit(name: str) -> None:
+def test_search_matches_reference_bit_for_bit(name: str, locality: bool) -> None:
+    """Both device node orders: the reference's, and the cell order (internal ids for memory,
+    original ids for results and for ties between equal distances)."""
     case = load_golden(f"search_{name}")
     arrays, ep, ml = case_arrays(case, name)
     metric = str(case["metric"])
     M = (arrays["links0"].shape[1] - 1) // 2
-    index = _index(arrays, ep, ml, metric, M)
+    index = _index(arrays, ep, ml, metric, M, locality)
     k = int(case["k"])
     for mi, mask, ef in iter_search_runs(case):
         index.reset_counters()
@@ -53,6 +57,24 @@ def test_every_arithmetic_mode_agrees_on_integer_data(mode: int) -> None:
         np.testing.assert_array_equal(ctr.sum(0).cpu().numpy(), case[f"ctr_m0_ef{ef}"])
 
 
+def test_device_mode_choice_equals_host_choice() -> None:
+    """The arithmetic chosen from device-resident queries is the one the host rules choose."""
+    import torch
+
+    case = load_golden("search_mix10k")
+    arrays, ep, ml = case_arrays(case, "mix10k")
+    g = _index(arrays, ep, ml, "l2", 16).device_graph
+    q = case["queries"].astype(np.float32)
+    batches = [q, q + 0.5, q * 3.0, q - 40.0, q * 40.0, q[:0]]
+    for b in batches:
+        for codes in (False, True):
+            if codes and g.codes is None:
+                g.attach_codes(np.asarray(arrays["vectors"], dtype=np.uint8))
+            dev = torch.from_numpy(np.ascontiguousarray(b, dtype=np.float64 if codes else np.float32)).cuda()
+            host = g.choose_mode(b, codes) if b.size else g.choose_mode_device(dev, codes)
+            assert g.choose_mode_device(dev, codes) == host
+
+
 def test_per_query_ef_matches_grouped_reference_calls() -> None:
     case = load_golden("search_mix10k")
     arrays, ep, ml = case_arrays(case, "mix10k")
@@ -65,15 +87,16 @@ def test_per_query_ef_matches_grouped_reference_calls() -> None:
     np.testing.assert_array_equal([st.distance_computations, st.hops], case["pq_ctr"])
 
 
+@pytest.mark.parametrize("locality", [False, True], ids=["reference_order", "cell_order"])
 @pytest.mark.parametrize("name", QUANT_CASES)
-def test_quantized_search_and_fused_rerank_match_reference(name: str) -> None:
+def test_quantized_search_and_fused_rerank_match_reference(name: str, locality: bool) -> None:
     from hnsw_engine_b200 import QuantizedIndex
 
     case = load_golden(f"quant_{name}")
     arrays, ep, ml = case_arrays(case, name)
     metric = str(case["metric"])
     M = (arrays["links0"].shape[1] - 1) // 2
-    qi = QuantizedIndex(_index(arrays, ep, ml, metric, M))
+    qi = QuantizedIndex(_index(arrays, ep, ml, metric, M, locality))
     for r in case["reranks"]:
         ids, dists = qi.batch_search(case["queries"], k=int(case["k"]), ef=int(case["ef"]), rerank=int(r))
         np.testing.assert_array_equal(ids, case[f"ids_r{r}"], err_msg=f"{name} r{r}")
