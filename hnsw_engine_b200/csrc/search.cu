@@ -58,6 +58,9 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_MINB_BYTES
 #define HB_MINB_BYTES 5
 #endif
+#ifndef HB_MINB_BYTES_FILT
+#define HB_MINB_BYTES_FILT 6
+#endif
 #ifndef HB_NB_EXACT
 #define HB_NB_EXACT 4
 #endif
@@ -94,8 +97,13 @@ __device__ unsigned long long hb_prof[8];
 
 template <int MODE>
 struct MinBlocks {
-    static constexpr int value =
-        MODE == 2 ? HB_MINB_BYTES : (MODE == 1 ? HB_MINB_EXACT : HB_MINB_F64);
+    // Filtered byte searches keep one more block resident: their candidate pushes are shared-memory
+    // work that hides less latency per warp.
+    template <bool FILT>
+    static constexpr int of() {
+        return MODE == 2 ? (FILT ? HB_MINB_BYTES_FILT : HB_MINB_BYTES)
+                         : (MODE == 1 ? HB_MINB_EXACT : HB_MINB_F64);
+    }
 };
 
 enum : int32_t { ST_VISITED = 1, ST_TIES = 2, ST_SPILL = 4 };
@@ -142,7 +150,8 @@ struct SearchParams {
     int32_t *ties;
     int32_t tie_cap;
     double *spill_d;
-    int32_t *spill_i;
+    int32_t *spill_i;       // original ids of spilled candidates
+    int32_t *spill_p;       // their internal ids (graphs in an internal order; else spill_i)
     int32_t spill_cap;
     int32_t s_cap;
     // learned early termination (layer 0, unfiltered): features every STOP_EVERY expansions
@@ -154,6 +163,7 @@ struct SearchParams {
     int32_t *trace_hops;    // (n_queries,) layer-0 expansions of the whole search
     int32_t trace_cap;
     int32_t trace_k;        // distances recorded per checkpoint (min(k, 16))
+    int32_t lane_rows;      // byte rows may use mark_score_lane_rows (see the host's choice)
 };
 
 constexpr int STOP_EVERY = 16;
@@ -183,7 +193,7 @@ __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filt
     size_t b = al16(size_t(result_slots(ef_cap)) * 8) +
                (two_ids ? 2 : 1) * al16(size_t(result_slots(ef_cap)) * 4) + al16(size_t(dim) * 8) +
                al16(size_t(dim) * 4) + al16(size_t(dim));
-    if (filtered) b += al16(size_t(s_cap + 1) * 8) + al16(size_t(s_cap + 1) * 4);
+    if (filtered) b += al16(size_t(s_cap + 1) * 8) + (two_ids ? 2 : 1) * al16(size_t(s_cap + 1) * 4);
     if (k_rerank > 0) b += al16(size_t(k_rerank + 1) * 8) + al16(size_t(k_rerank + 1) * 4);
     return b;
 }
@@ -197,7 +207,8 @@ struct Ctx {
     float *qf;
     uint32_t *q4;  // query bytes, four per word (byte mode)
     double *Sd;
-    int32_t *Si;
+    int32_t *Si;  // candidates: original ids
+    int32_t *Sp;  // candidates: internal ids (the same array as Si unless the order differs)
     double *Ad;
     int32_t *Ai;
     int32_t *vis;
@@ -207,6 +218,7 @@ struct Ctx {
     int32_t *ties;
     double *spd;
     int32_t *spi;
+    int32_t *spp;
     long long ndist, nhops;  // uniform across the warp
     int32_t status;          // uniform across the warp
     int32_t q;               // query row
@@ -235,11 +247,6 @@ __device__ __forceinline__ bool pair_lt_raw(double da, int32_t ia, double db, in
     return da < db || (da == db && ia < ib);
 }
 
-// (distance, original id) order of two entries given by internal ids.
-__device__ __forceinline__ bool pair_lt(const SearchParams &P, double da, int32_t ia, double db,
-                                        int32_t ib) {
-    return da < db || (da == db && orig_id(P, ia) < orig_id(P, ib));
-}
 
 // ---------------------------------------------------------------------------------------- sorted
 // Entries of the ascending array [0, m) strictly below (d, id).
@@ -268,10 +275,10 @@ __device__ __forceinline__ int sorted_rank(const double *Ad, const int32_t *Ai, 
 }
 
 // Entries of the descending array [0, m) strictly above (d, id).
-__device__ __forceinline__ int count_above(const SearchParams &P, const double *Ad, const int32_t *Ai, int m, double d,
+__device__ __forceinline__ int count_above(const double *Ad, const int32_t *Ai, int m, double d,
                                            int32_t id, int lane) {
     int c = 0;
-    for (int i = lane; i < m; i += 32) c += pair_lt(P, d, id, Ad[i], Ai[i]);
+    for (int i = lane; i < m; i += 32) c += pair_lt_raw(d, id, Ad[i], Ai[i]);
     return __reduce_add_sync(FULL, c);
 }
 
@@ -298,21 +305,24 @@ __device__ __forceinline__ void shift_up(double *Ad, int32_t *Ai, int pos, int m
     }
 }
 
-// Move [pos + 1, m) to [pos, m - 1), lowest chunk first.
-__device__ __forceinline__ void shift_down(double *Ad, int32_t *Ai, int pos, int m, int lane) {
+// Move [pos + 1, m) to [pos, m - 1), lowest chunk first (Ap: an optional third array).
+__device__ __forceinline__ void shift_down(double *Ad, int32_t *Ai, int pos, int m, int lane,
+                                           int32_t *Ap = nullptr) {
     for (int base = pos; base < m - 1; base += 32) {
         int i = base + lane;
         bool act = i < m - 1;
         double d = 0.0;
-        int32_t id = 0;
+        int32_t id = 0, ip = 0;
         if (act) {
             d = Ad[i + 1];
             id = Ai[i + 1];
+            if (Ap) ip = Ap[i + 1];
         }
         __syncwarp();
         if (act) {
             Ad[i] = d;
             Ai[i] = id;
+            if (Ap) Ap[i] = ip;
         }
         __syncwarp();
     }
@@ -1093,11 +1103,12 @@ struct Cands {
 };
 
 __device__ __forceinline__ void spill_push(const SearchParams &P, Ctx &C, Cands &K, double d,
-                                           int32_t id) {
+                                           int32_t id, int32_t ip) {
     if (K.g < P.spill_cap) {
         if (C.lane == 0) {
             C.spd[K.g] = d;
             C.spi[K.g] = id;
+            if (C.spp != C.spi) C.spp[K.g] = ip;
         }
         K.g++;
     } else {
@@ -1105,26 +1116,30 @@ __device__ __forceinline__ void spill_push(const SearchParams &P, Ctx &C, Cands 
     }
 }
 
+// id: original id (ordering); ip: internal id (expansion).
 __device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &K, double d,
-                                          int32_t id) {
-    if (K.g > 0 && !pair_lt(P, d, id, K.gd, K.gi)) {  // not below the spill minimum
-        spill_push(P, C, K, d, id);
+                                          int32_t id, int32_t ip) {
+    int32_t *sp = C.Sp != C.Si ? C.Sp : nullptr;
+    if (K.g > 0 && !pair_lt_raw(d, id, K.gd, K.gi)) {  // not below the spill minimum
+        spill_push(P, C, K, d, id, ip);
         return;
     }
-    const int pos = count_above(P, C.Sd, C.Si, K.s, d, id, C.lane);
-    shift_up(C.Sd, C.Si, pos, K.s, C.lane);
+    const int pos = count_above(C.Sd, C.Si, K.s, d, id, C.lane);
+    shift_up(C.Sd, C.Si, pos, K.s, C.lane, sp);
     if (C.lane == 0) {
         C.Sd[pos] = d;
         C.Si[pos] = id;
+        if (sp) sp[pos] = ip;
     }
     __syncwarp();
     K.s++;
     if (K.s > P.s_cap) {  // move the maximum to the spill; it becomes the spill minimum
         const double md = C.Sd[0];
         const int32_t mi = C.Si[0];
-        shift_down(C.Sd, C.Si, 0, K.s, C.lane);
+        const int32_t mp = sp ? sp[0] : mi;
+        shift_down(C.Sd, C.Si, 0, K.s, C.lane, sp);
         K.s--;
-        spill_push(P, C, K, md, mi);
+        spill_push(P, C, K, md, mi, mp);
         K.gd = md;
         K.gi = mi;
     }
@@ -1135,37 +1150,41 @@ __device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &
 __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune, double Wp) {
     const int lane = C.lane;
     const int B = max(1, P.s_cap / 2);
+    int32_t *sp = C.Sp != C.Si ? C.Sp : nullptr;
     int s = 0;
     for (int base = 0; base < K.g; base += 32) {
         const int i = base + lane;
         double d = 0.0;
-        int32_t id = 0;
+        int32_t id = 0, ip = 0;
         bool v = i < K.g;
         if (v) {
             d = C.spd[i];
             id = C.spi[i];
+            ip = sp ? C.spp[i] : id;
             if (prune && d > Wp) v = false;
         }
-        uint32_t cm = __ballot_sync(FULL, v && (s < B || pair_lt(P, d, id, C.Sd[0], C.Si[0])));
+        uint32_t cm = __ballot_sync(FULL, v && (s < B || pair_lt_raw(d, id, C.Sd[0], C.Si[0])));
         while (cm) {
             const int j = __ffs(cm) - 1;
             cm &= cm - 1;
             const double xd = __shfl_sync(FULL, d, j);
             const int32_t xi = __shfl_sync(FULL, id, j);
-            if (!(s < B || pair_lt(P, xd, xi, C.Sd[0], C.Si[0]))) continue;
-            const int pos = count_above(P, C.Sd, C.Si, s, xd, xi, lane);
-            shift_up(C.Sd, C.Si, pos, s, lane);
+            const int32_t xp = sp ? __shfl_sync(FULL, ip, j) : xi;
+            if (!(s < B || pair_lt_raw(xd, xi, C.Sd[0], C.Si[0]))) continue;
+            const int pos = count_above(C.Sd, C.Si, s, xd, xi, lane);
+            shift_up(C.Sd, C.Si, pos, s, lane, sp);
             if (lane == 0) {
                 C.Sd[pos] = xd;
                 C.Si[pos] = xi;
+                if (sp) sp[pos] = xp;
             }
             __syncwarp();
             s++;
             if (s > B) {
-                shift_down(C.Sd, C.Si, 0, s, lane);
+                shift_down(C.Sd, C.Si, 0, s, lane, sp);
                 s--;
             }
-            if (s == B) cm &= __ballot_sync(FULL, pair_lt(P, d, id, C.Sd[0], C.Si[0]));
+            if (s == B) cm &= __ballot_sync(FULL, pair_lt_raw(d, id, C.Sd[0], C.Si[0]));
         }
     }
     // Compact the spill: keep entries not selected (above S's maximum) and not pruned.
@@ -1177,12 +1196,13 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
     for (int base = 0; base < K.g; base += 32) {
         const int i = base + lane;
         double d = 0.0;
-        int32_t id = 0;
+        int32_t id = 0, ip = 0;
         bool keep = false;
         if (i < K.g) {
             d = C.spd[i];
             id = C.spi[i];
-            keep = !(prune && d > Wp) && pair_lt(P, td, ti, d, id);
+            ip = sp ? C.spp[i] : id;
+            keep = !(prune && d > Wp) && pair_lt_raw(td, ti, d, id);
         }
         const uint32_t km = __ballot_sync(FULL, keep);
         __syncwarp();
@@ -1190,7 +1210,8 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
             const int o = w + __popc(km & ((1u << lane) - 1u));
             C.spd[o] = d;
             C.spi[o] = id;
-            if (pair_lt(P, d, id, md, mi)) {
+            if (sp) C.spp[o] = ip;
+            if (pair_lt_raw(d, id, md, mi)) {
                 md = d;
                 mi = id;
             }
@@ -1202,7 +1223,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
     for (int o = 16; o > 0; o >>= 1) {
         const double od = __shfl_xor_sync(FULL, md, o);
         const int32_t oi = __shfl_xor_sync(FULL, mi, o);
-        if (pair_lt(P, od, oi, md, mi)) {
+        if (pair_lt_raw(od, oi, md, mi)) {
             md = od;
             mi = oi;
         }
@@ -1225,7 +1246,8 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
     bitmap_begin(P, C, e0);
     if (lane == 0) {  // candidates hold internal ids; results hold both
         C.Sd[0] = d0;
-        C.Si[0] = e0;
+        C.Si[0] = o0;
+        C.Sp[0] = e0;
         if (is_allowed(P.allowed, e0)) {
             C.Rd[0] = d0;
             C.Ri[0] = o0;
@@ -1245,7 +1267,7 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
             if (K.s == 0) break;
         }
         const double dc = C.Sd[K.s - 1];
-        const int32_t c = C.Si[K.s - 1];
+        const int32_t c = C.Sp[K.s - 1];
         K.s--;
         if (r == ef && dc > W) break;
         C.nhops++;
@@ -1264,10 +1286,10 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
                 am &= am - 1;
                 const double d = __shfl_sync(FULL, dj, j);
                 const int32_t id = __shfl_sync(FULL, e, j);
+                const int32_t ido = __shfl_sync(FULL, eo, j);
                 if (!(r < ef || d < W)) continue;
-                cand_push(P, C, K, d, id);
+                cand_push(P, C, K, d, ido, id);
                 if (is_allowed(P.allowed, id)) {
-                    const int32_t ido = __shfl_sync(FULL, eo, j);  // uniform branch
                     const int pos = count_below(C.Rd, C.Ri, r, d, ido, lane);
                     shift_up(C.Rd, C.Ri, pos, r, lane, C.Rp != C.Ri ? C.Rp : nullptr);
                     if (lane == 0) {
@@ -1323,7 +1345,8 @@ __device__ int rerank_epilogue(const SearchParams &P, Ctx &C, int m) {
 
 // --------------------------------------------------------------------------------------- kernel
 template <int MODE, bool U8, bool FILT>
-__global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kernel(const SearchParams P) {
+__global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>())
+    search_kernel(const SearchParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -1350,11 +1373,17 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
     p += al16(size_t(P.dim));
     C.Sd = nullptr;
     C.Si = nullptr;
+    C.Sp = nullptr;
     if (FILT) {
         C.Sd = reinterpret_cast<double *>(p);
         p += al16(size_t(P.s_cap + 1) * 8);
         C.Si = reinterpret_cast<int32_t *>(p);
         p += al16(size_t(P.s_cap + 1) * 4);
+        C.Sp = C.Si;
+        if (two_ids) {
+            C.Sp = reinterpret_cast<int32_t *>(p);
+            p += al16(size_t(P.s_cap + 1) * 4);
+        }
     }
     C.Ad = reinterpret_cast<double *>(p);
     p += rerank ? al16(size_t(P.k + 1) * 8) : 0;
@@ -1378,7 +1407,8 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::value) search_kerne
     C.ties = P.ties + slot * P.tie_cap;
     C.spd = FILT ? P.spill_d + slot * P.spill_cap : nullptr;
     C.spi = FILT ? P.spill_i + slot * P.spill_cap : nullptr;
-    C.lane_rows = (P.dim & 15) == 0 && P.dim <= 128;
+    C.spp = FILT ? (two_ids ? P.spill_p + slot * P.spill_cap : C.spi) : nullptr;
+    C.lane_rows = P.lane_rows && (P.dim & 15) == 0 && P.dim <= 128;
 
     for (;;) {
         int w = 0;
@@ -1552,7 +1582,7 @@ struct Handle {
     Buffer counters;  // queue, n_failed, n_list
     Buffer status;
     Buffer qlist[2];  // retry work lists (ping-pong)
-    Buffer vis, ties, spill_d, spill_i, vbits, vlist;
+    Buffer vis, ties, spill_d, spill_i, spill_p, vbits, vlist;
     bool bits_dirty = false;  // a launch failed mid-flight: bitmaps must be re-zeroed
     int32_t *host_pinned = nullptr;  // 4 ints
     long long launches = 0;
@@ -1689,6 +1719,7 @@ void hnsw_b200_close(void *handle) {
     h->ties.release();
     h->spill_d.release();
     h->spill_i.release();
+    h->spill_p.release();
     if (h->host_pinned) cudaFreeHost(h->host_pinned);
     delete h;
 }
@@ -1796,6 +1827,9 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.trace_hops = a->trace_hops;
     P.trace_cap = a->trace_cap;
     P.trace_k = 16;
+    // One lane per neighbour's row: a win unless the filter is very selective, where most rows it
+    // would fetch early belong to neighbours already visited.
+    P.lane_rows = (!filt || p >= 0.05) ? 1 : 0;
 
     int32_t n_work = nq;
     const int32_t *qlist = nullptr;
@@ -1816,6 +1850,8 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         if (filt) {
             if (int rc = h.spill_d.ensure(size_t(slots) * spill_cap * sizeof(double))) return rc;
             if (int rc = h.spill_i.ensure(size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
+            if (g.node_ids)
+                if (int rc = h.spill_p.ensure(size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
         }
         P.vbits = static_cast<uint32_t *>(h.vbits.ptr);
         P.vbits_stride = vbits_stride;
@@ -1829,6 +1865,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         P.tie_cap = tie_cap;
         P.spill_d = static_cast<double *>(h.spill_d.ptr);
         P.spill_i = static_cast<int32_t *>(h.spill_i.ptr);
+        P.spill_p = static_cast<int32_t *>(h.spill_p.ptr);
         P.spill_cap = spill_cap;
         P.qlist = qlist;
         P.n_work = n_work;
@@ -2040,6 +2077,7 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     P.trace_hops = a->trace_hops;
     P.trace_cap = a->trace_cap;
     P.trace_k = 16;
+    P.lane_rows = 1;
     int rc = 0;
     if (mode == MODE_BYTES)
         rc = launch_one_noalloc<MODE_BYTES, true>(P, smem_block, blocks, s);

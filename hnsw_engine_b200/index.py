@@ -299,14 +299,24 @@ class HNSWIndex:
 
     def batch_search(
         self, queries: Any, k: int = 10, ef: Any = None, filter: ArrayLike | None = None,
-        stop: Any = None,
+        stop: Any = None, exact_below: float | None = None,
     ) -> tuple[Any, Any]:
         """:meth:`search` for each row of ``(nq, dim)`` queries (reference ``index.py:275-292``).
 
         ``ef`` may be one integer or an array of one efSearch per query. Torch device queries give
-        device results (no host round trip); host queries give numpy results. Extension: ``stop``,
-        a trained :class:`~hnsw_engine_b200.learned_stop.StopNetwork`, ends each unfiltered query
-        early once the network predicts no further recall gain (``ef`` is then the cap).
+        device results (no host round trip); host queries give numpy results.
+
+        Extensions:
+
+        * ``stop``: a trained :class:`~hnsw_engine_b200.learned_stop.StopNetwork` ends each
+          unfiltered query early once the network predicts no further recall gain (``ef`` is then
+          the cap).
+        * ``exact_below``: a selectivity planner. When the filter allows fewer than this share of
+          the nodes, the batch is answered by the tensor-core exact k-NN over the allowed rows
+          instead of the graph walk, which must pass through about 1/share nodes per result
+          (the policy of the reference's ``benchmarks/run_filtered.py:76-106``). The results are
+          then the exact neighbours among the allowed nodes, as ``oracle.exact_search`` gives them;
+          the distance counter adds one per (query, allowed node).
         """
         k_valid, ef_valid = self._check_search_args(k, ef)
         allowed = self._check_filter(filter)
@@ -327,9 +337,34 @@ class HNSWIndex:
             if on_device:
                 return torch.from_numpy(ids).to(queries.device), torch.from_numpy(dists).to(queries.device)
             return ids, dists
+        if allowed is not None and exact_below is not None and allowed.mean() < float(exact_below):
+            return self._exact_subset(prepared, k_valid, allowed, keep_device=on_device)
         ids_t, dists_t = self._run(prepared, k_valid, ef_valid, allowed, keep_device=on_device,
                                    stop=stop)
         return ids_t, dists_t
+
+    def _exact_subset(self, prepared: Any, k: int, allowed: NDArray[np.bool_],
+                      keep_device: bool = False) -> tuple[Any, Any]:
+        """Exact k nearest allowed nodes (ties to the lower id), padded with -1 / inf."""
+        from .exact_knn import exact_search
+
+        g = self.device_graph
+        dev = g.device
+        sub = torch.from_numpy(np.flatnonzero(allowed)).to(dev)
+        q = prepared if isinstance(prepared, torch.Tensor) else torch.from_numpy(prepared)
+        q = q.to(device=dev, dtype=torch.float32).contiguous()
+        nq = q.shape[0]
+        kk = min(k, int(sub.numel()))
+        ids = torch.full((nq, k), -1, dtype=torch.int64, device=dev)
+        dists = torch.full((nq, k), float("inf"), dtype=torch.float64, device=dev)
+        if nq and kk:
+            sub_ids, sub_d = exact_search(g.vectors[sub].contiguous(), q, kk, self._metric)
+            ids[:, :kk] = sub[sub_ids]
+            dists[:, :kk] = sub_d
+        self._counters[0] += nq * int(sub.numel())
+        if keep_device:
+            return ids, dists
+        return ids.cpu().numpy(), dists.cpu().numpy()
 
     def _run(self, prepared: Any, k: int, ef: Any, allowed: NDArray[np.bool_] | None,
              keep_device: bool = False, stop: Any = None) -> tuple[Any, Any]:

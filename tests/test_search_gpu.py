@@ -208,3 +208,31 @@ def test_million_node_graphs_match_oracle(name: str) -> None:
     q = prepare(graphs.workload_queries(name, nq=96), metric)
     ef = synthetic.per_query_ef(96, seed=6, low=32, high=512)
     _oracle_compare(arrays, ep, ml, metric, q, 10, ef)
+
+
+@pytest.mark.parametrize("allowed_count", [3, 100])
+def test_selective_filter_planner_returns_the_exact_allowed_neighbors(allowed_count: int) -> None:
+    """Below the planner's selectivity the batch is answered exactly over the allowed rows: ids and
+    distances equal the CPU oracle's exact search of that subset, padded when fewer than k."""
+    from oracle import exact
+
+    case = load_golden("search_mix10k")
+    arrays, ep, ml = case_arrays(case, "mix10k")
+    index = _index(arrays, ep, ml, "l2", 16)
+    rng = np.random.default_rng(3)
+    mask = np.zeros(arrays["vectors"].shape[0], dtype=bool)
+    mask[rng.choice(mask.size, allowed_count, replace=False)] = True
+    q = case["queries"][:64]
+    index.reset_counters()
+    ids, dists = index.batch_search(q, k=10, ef=64, filter=mask, exact_below=0.05)
+    sub = np.flatnonzero(mask)
+    kk = min(10, allowed_count)
+    o_ids, o_d = exact.exact_search(np.asarray(arrays["vectors"])[sub], q, kk, "l2")
+    np.testing.assert_array_equal(ids[:, :kk], sub[o_ids])
+    np.testing.assert_array_equal(dists[:, :kk], o_d)
+    assert (ids[:, kk:] == -1).all() and np.isinf(dists[:, kk:]).all()
+    assert index.distance_computations == q.shape[0] * allowed_count
+    # above the cutoff the graph walk answers, as the reference does
+    g_ids, _ = index.batch_search(q, k=10, ef=64, filter=mask, exact_below=allowed_count / mask.size)
+    ref_ids, _ = index.batch_search(q, k=10, ef=64, filter=mask)
+    np.testing.assert_array_equal(g_ids, ref_ids)
