@@ -118,6 +118,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                                   ctypes.c_void_p]),
     "hnsw_b200_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
     "hnsw_b200_last_error": (ctypes.c_char_p, []),
+    "hnsw_b200_validate_scratch_bytes": (ctypes.c_int64, [ctypes.c_int64]),
+    "hnsw_b200_validate_graph": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.c_void_p, ctypes.c_int32,
+                                                ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                                ctypes.c_void_p]),
     "hnsw_b200_version": (ctypes.c_char_p, []),
 }
 

@@ -66,6 +66,7 @@ class DeviceGraph:
         metric: str,
         device: str | torch.device = "cuda",
         locality: bool | None = None,
+        validate_M: int | None = None,
     ) -> None:
         self.lib = _lib.load()
         self.device = torch.device(device)
@@ -114,10 +115,31 @@ class DeviceGraph:
         self.order: torch.Tensor | None = None  # internal node -> original id (None: identity)
         self._order_host: NDArray[np.int64] | None = None
         self._internal: dict[str, Any] = {}
+        if validate_M is not None:  # before anything follows the links
+            self._validate_on_device(arrays["levels"], int(validate_M))
         if self.locality:
             self._build_internal_order()
         self._handle = ctypes.c_void_p()
         self._open()
+
+    def _validate_on_device(self, levels: NDArray[np.int64], M: int) -> None:
+        """The checks of the reference's _validate_native on the uploaded arrays (one kernel pass);
+        raises its ValueError for the first failed check."""
+        from .validation import device_validation_message
+
+        dev = self.device
+        with torch.cuda.device(dev):
+            lv = to_device(levels, torch.int64, dev)
+            scratch = torch.empty(int(self.lib.hnsw_b200_validate_scratch_bytes(self.rows)),
+                                  dtype=torch.uint8, device=dev)
+            flags = ctypes.c_uint32(0)
+            g = self._graph_struct()
+            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+            _lib.check(self.lib.hnsw_b200_validate_graph(ctypes.byref(g), _dev_ptr(lv), M,
+                                                         _dev_ptr(scratch), ctypes.byref(flags), stream))
+        message = device_validation_message(int(flags.value), M)
+        if message is not None:
+            raise ValueError(message)
 
     # ------------------------------------------------------------------------ node order
     def _build_internal_order(self) -> None:

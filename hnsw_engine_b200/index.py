@@ -175,15 +175,17 @@ class HNSWIndex:
     def _attach(self, arrays: dict[str, NDArray[Any]], entry_point: int, max_level: int,
                 validate: bool) -> None:
         check_native_shapes(arrays, self._dim, self._M)
-        if validate:
+        size = int(arrays["vectors"].shape[0])
+        if validate and size == 0:
             validate_native(arrays, entry_point, max_level, self._M)
         self._arrays = {name: arrays[name] for name in NATIVE_ARRAYS}
-        self._size = int(arrays["vectors"].shape[0])
+        if size:
+            # validate: the reference's checks, run on the GPU over the uploaded arrays
+            self._graph = DeviceGraph(self._arrays, entry_point, max_level, self._metric, self._device,
+                                      locality=self._locality, validate_M=self._M if validate else None)
+        self._size = size
         self._entry_point = entry_point
         self._max_level = max_level
-        if self._size:
-            self._graph = DeviceGraph(self._arrays, entry_point, max_level, self._metric, self._device,
-                                      locality=self._locality)
 
     # ---------------------------------------------------------------------- properties
     @property

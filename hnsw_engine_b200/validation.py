@@ -159,3 +159,23 @@ def validate_native(arrays: dict[str, NDArray[Any]], entry_point: int, max_level
     layer_of_row = np.arange(rows) - np.repeat(starts, sizes) + 1
     if (levels[targets] < np.repeat(layer_of_row, count_up)).any():
         raise ValueError("an upper-layer link points to a node absent from that layer")
+
+
+# Messages of validate_native, in its order of checks, for the failure bits of the on-device
+# validator (hnsw_b200_validate_graph, HNSW_B200_BAD_* in include/hnsw_b200.h).
+def device_validation_message(flags: int, M: int) -> str | None:
+    """The message validate_native raises for the first failed check, or None if none failed."""
+    messages = (
+        "negative node level",
+        "the entry point is not a node of the top layer",
+        f"layer 0: link counts outside [0, {2 * M}]",
+        "layer 0: a link points outside the graph",
+        "upper-layer rows of the nodes overlap or leave gaps",
+        f"upper layers: link counts outside [0, {M}]",
+        "upper layers: a link points outside the graph",
+        "an upper-layer link points to a node absent from that layer",
+    )
+    for bit, message in enumerate(messages):
+        if flags >> bit & 1:
+            return message
+    return None

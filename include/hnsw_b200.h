@@ -18,6 +18,8 @@
  *                          _rerank_batch (:506-530), fused into one launch; extended with a
  *                          per-query ef array and a filter on code-space searches.
  *   hnsw_b200_exact_knn <- oracle.exact_search (src/hnsw_engine/oracle.py:35-126).
+ *   hnsw_b200_validate_graph <- numba_engine._validate_native (numba_engine.py:878-915), on the
+ *                          uploaded arrays.
  *   hnsw_b200_mlp_*     <- no reference counterpart (the learned early-termination network).
  */
 #ifndef HNSW_B200_H
@@ -201,6 +203,26 @@ int64_t hnsw_b200_last_launches(void *handle);
 
 /* Thread-local text of the last error. */
 const char *hnsw_b200_last_error(void);
+
+/* Validation of a graph's uploaded arrays on the GPU: the checks of the reference's
+ * _validate_native (numba_engine.py:878-915) -- node levels, entry point on the top layer, link
+ * counts within capacity, link targets inside the graph, upper-layer rows tiling [0, rows),
+ * upper-layer links landing on nodes present on that layer. levels: (n,) int64 device array.
+ * scratch: device memory of hnsw_b200_validate_scratch_bytes(graph->rows) bytes. flags_out (host)
+ * receives the failed checks as HNSW_B200_BAD_* bits; 0 means valid. The bits are numbered in the
+ * order the host validator checks, so the lowest set bit names the error it would raise.
+ * Synchronises the stream. */
+#define HNSW_B200_BAD_LEVEL 1u      /* a negative node level */
+#define HNSW_B200_BAD_ENTRY 2u      /* the entry point (or max_level) is not the top layer's */
+#define HNSW_B200_BAD_COUNT0 4u     /* a layer-0 link count outside [0, 2M] */
+#define HNSW_B200_BAD_LINK0 8u      /* a layer-0 link outside the graph */
+#define HNSW_B200_BAD_ROWS 16u      /* upper-layer rows overlap or leave gaps */
+#define HNSW_B200_BAD_COUNT_UP 32u  /* an upper-layer link count outside [0, M] */
+#define HNSW_B200_BAD_LINK_UP 64u   /* an upper-layer link outside the graph */
+#define HNSW_B200_BAD_LAYER 128u    /* an upper-layer link to a node absent from that layer */
+int64_t hnsw_b200_validate_scratch_bytes(int64_t rows);
+int hnsw_b200_validate_graph(const hnsw_b200_graph_t *graph, const int64_t *levels, int32_t M,
+                             void *scratch, uint32_t *flags_out, void *stream);
 
 /* Library version string. */
 const char *hnsw_b200_version(void);
