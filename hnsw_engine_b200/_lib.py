@@ -119,6 +119,12 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "hnsw_b200_last_launches": (ctypes.c_int64, [ctypes.c_void_p]),
     "hnsw_b200_last_error": (ctypes.c_char_p, []),
     "hnsw_b200_validate_scratch_bytes": (ctypes.c_int64, [ctypes.c_int64]),
+    "hnsw_b200_quant_scratch_bytes": (ctypes.c_int64, [ctypes.c_int32]),
+    "hnsw_b200_quant_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p,
+                                             ctypes.c_void_p]),
+    "hnsw_b200_quant_encode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_validate_graph": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.c_void_p, ctypes.c_int32,
                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                                 ctypes.c_void_p]),

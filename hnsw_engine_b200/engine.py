@@ -235,9 +235,11 @@ class DeviceGraph:
         with torch.cuda.device(self.device):
             _lib.check(self.lib.hnsw_b200_open(ctypes.byref(g), ctypes.byref(self._handle)))
 
-    def attach_codes(self, codes: NDArray[np.uint8]) -> None:
-        """Upload scalar-quantizer codes (n, dim) uint8 for code-space searches."""
-        if codes.shape != (self.n, self.dim) or codes.dtype != np.uint8:
+    def attach_codes(self, codes: NDArray[np.uint8] | torch.Tensor) -> None:
+        """Attach scalar-quantizer codes (n, dim) uint8 (host array or device tensor, original node
+        order) for code-space searches."""
+        is_u8 = codes.dtype == (torch.uint8 if isinstance(codes, torch.Tensor) else np.uint8)
+        if tuple(codes.shape) != (self.n, self.dim) or not is_u8:
             raise ValueError(f"codes must be uint8 with shape {(self.n, self.dim)}")
         with torch.cuda.device(self.device):
             self.codes = to_device(codes, torch.uint8, self.device)

@@ -19,10 +19,13 @@ from __future__ import annotations
 from dataclasses import dataclass
 from typing import Any
 
+import ctypes
+
 import numpy as np
 import torch
 from numpy.typing import ArrayLike, NDArray
 
+from . import _lib
 from .index import HNSWIndex
 from .validation import as_matrix, check_int
 
@@ -47,10 +50,49 @@ class ScalarQuantizer:
         step = 1.0 if (lossless or widest == 0.0) else widest / (CODE_LEVELS - 1)
         return cls(low, step)
 
+    @classmethod
+    def fit_device(cls, vectors: torch.Tensor) -> ScalarQuantizer:
+        """:meth:`fit` of float32 rows resident on a GPU: one pass of the library's column
+        statistics kernel (minima, maxima, integrality), then the same step rule."""
+        n, dim = vectors.shape
+        if n == 0:
+            raise ValueError("cannot fit a quantizer on zero vectors")
+        lib = _lib.load()
+        dev = vectors.device
+        x = vectors.to(torch.float32).contiguous()
+        with torch.cuda.device(dev):
+            lo = torch.empty(dim, dtype=torch.float64, device=dev)
+            hi = torch.empty(dim, dtype=torch.float64, device=dev)
+            scratch = torch.empty(int(lib.hnsw_b200_quant_scratch_bytes(dim)), dtype=torch.uint8, device=dev)
+            integer = ctypes.c_int32(0)
+            stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+            _lib.check(lib.hnsw_b200_quant_stats(x.data_ptr(), n, dim, lo.data_ptr(), hi.data_ptr(),
+                                                 ctypes.byref(integer), scratch.data_ptr(), stream))
+        low = lo.cpu().numpy()
+        widest = float((hi.cpu().numpy() - low).max())
+        lossless = bool(integer.value) and widest <= CODE_LEVELS - 1
+        step = 1.0 if (lossless or widest == 0.0) else widest / (CODE_LEVELS - 1)
+        return cls(low, step)
+
     def encode(self, vectors: ArrayLike) -> NDArray[np.uint8]:
         x = np.asarray(vectors, dtype=np.float64)
         codes = np.clip(np.rint((x - self.offset) / self.step), 0, CODE_LEVELS - 1)
         return np.ascontiguousarray(codes, dtype=np.uint8)
+
+    def encode_device(self, vectors: torch.Tensor) -> torch.Tensor:
+        """:meth:`encode` of float32 rows resident on a GPU (the same float64 arithmetic)."""
+        lib = _lib.load()
+        dev = vectors.device
+        x = vectors.to(torch.float32).contiguous()
+        n, dim = x.shape
+        with torch.cuda.device(dev):
+            codes = torch.empty((n, dim), dtype=torch.uint8, device=dev)
+            if n:
+                off = torch.from_numpy(np.ascontiguousarray(self.offset, dtype=np.float64)).to(dev)
+                stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+                _lib.check(lib.hnsw_b200_quant_encode(x.data_ptr(), n, dim, off.data_ptr(),
+                                                      float(self.step), codes.data_ptr(), stream))
+        return codes
 
     def decode(self, codes: NDArray[np.uint8]) -> NDArray[np.float64]:
         return self.offset + self.step * codes.astype(np.float64)
@@ -79,14 +121,24 @@ class QuantizedIndex:
         if len(index) == 0:
             raise ValueError("cannot quantize an empty index")
         self._index = index
-        vectors = index.native_arrays()["vectors"]
-        self.quantizer = ScalarQuantizer.fit(vectors)
-        self.codes = self.quantizer.encode(vectors)
-        index.device_graph.attach_codes(self.codes)
+        # fit and encode on the GPU, over the rows already resident for searching
+        g = index.device_graph
+        self.quantizer = ScalarQuantizer.fit_device(g.vectors)
+        self._codes_device = self.quantizer.encode_device(g.vectors)
+        self._n = len(index)
+        g.attach_codes(self._codes_device)
+        self._codes_host: NDArray[np.uint8] | None = None
+
+    @property
+    def codes(self) -> NDArray[np.uint8]:
+        """The (n, dim) uint8 codes (the reference's ``QuantizedIndex.codes``)."""
+        if self._codes_host is None:
+            self._codes_host = self._codes_device.cpu().numpy()
+        return self._codes_host
 
     @property
     def code_bytes(self) -> int:
-        return int(self.codes.nbytes)
+        return int(self._codes_device.numel())
 
     @property
     def vector_bytes(self) -> int:
@@ -102,7 +154,7 @@ class QuantizedIndex:
         search collects ``max(R, k)`` candidates (with at least that ``ef``) and returns the best
         ``k`` by exact distance, ties to the lower id.
         """
-        if len(self._index) != self.codes.shape[0]:
+        if len(self._index) != self._n:
             raise ValueError("the index changed after quantization; build a new QuantizedIndex")
         k_valid, ef_valid = self._index._check_search_args(k, ef)
         r = check_int(rerank, "rerank", minimum=0)

@@ -20,6 +20,7 @@
  *   hnsw_b200_exact_knn <- oracle.exact_search (src/hnsw_engine/oracle.py:35-126).
  *   hnsw_b200_validate_graph <- numba_engine._validate_native (numba_engine.py:878-915), on the
  *                          uploaded arrays.
+ *   hnsw_b200_quant_*   <- quantization.ScalarQuantizer.fit / encode (quantization.py:37-59).
  *   hnsw_b200_mlp_*     <- no reference counterpart (the learned early-termination network).
  */
 #ifndef HNSW_B200_H
@@ -221,6 +222,19 @@ const char *hnsw_b200_last_error(void);
 #define HNSW_B200_BAD_LINK_UP 64u   /* an upper-layer link outside the graph */
 #define HNSW_B200_BAD_LAYER 128u    /* an upper-layer link to a node absent from that layer */
 int64_t hnsw_b200_validate_scratch_bytes(int64_t rows);
+
+/* Scalar quantizer on the GPU (ScalarQuantizer.fit / encode, quantization.py:37-59).
+ * hnsw_b200_quant_stats: per-dimension minima lo and maxima hi (float64, device, dim each) of
+ * float32 rows, and *integer_valued (host) = 1 if every value is an integer; scratch: device
+ * memory of hnsw_b200_quant_scratch_bytes(dim) bytes; synchronises the stream. The caller derives
+ * offset = lo and the step exactly as fit does.
+ * hnsw_b200_quant_encode: codes[i][j] = clip(rint((double(x[i][j]) - offset[j]) / step), 0, 255),
+ * float64 arithmetic as the reference's encode (codes bit for bit equal). */
+int64_t hnsw_b200_quant_scratch_bytes(int32_t dim);
+int hnsw_b200_quant_stats(const float *vectors, int64_t n, int32_t dim, double *lo, double *hi,
+                          int32_t *integer_valued, void *scratch, void *stream);
+int hnsw_b200_quant_encode(const float *vectors, int64_t n, int32_t dim, const double *offset,
+                           double step, uint8_t *codes, void *stream);
 int hnsw_b200_validate_graph(const hnsw_b200_graph_t *graph, const int64_t *levels, int32_t M,
                              void *scratch, uint32_t *flags_out, void *stream);
 

@@ -236,3 +236,22 @@ def test_selective_filter_planner_returns_the_exact_allowed_neighbors(allowed_co
     g_ids, _ = index.batch_search(q, k=10, ef=64, filter=mask, exact_below=allowed_count / mask.size)
     ref_ids, _ = index.batch_search(q, k=10, ef=64, filter=mask)
     np.testing.assert_array_equal(g_ids, ref_ids)
+
+
+@pytest.mark.parametrize("name", QUANT_CASES)
+def test_device_quantizer_equals_the_reference_codes(name: str) -> None:
+    """Fit and encode on the GPU give the reference's offset, step and codes bit for bit."""
+    from hnsw_engine_b200 import QuantizedIndex
+    from hnsw_engine_b200.quantization import ScalarQuantizer
+
+    case = load_golden(f"quant_{name}")
+    arrays, ep, ml = case_arrays(case, name)
+    metric = str(case["metric"])
+    M = (arrays["links0"].shape[1] - 1) // 2
+    qi = QuantizedIndex(_index(arrays, ep, ml, metric, M))
+    np.testing.assert_array_equal(qi.quantizer.offset, case["offset"])  # the reference's fit
+    assert qi.quantizer.step == float(case["step"])
+    vectors = np.asarray(qi._index.native_arrays()["vectors"])
+    np.testing.assert_array_equal(qi.codes, ScalarQuantizer(case["offset"], float(case["step"])).encode(vectors))
+    if "codes" in case:  # the reference's own codes
+        np.testing.assert_array_equal(qi.codes, case["codes"])
