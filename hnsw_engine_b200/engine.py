@@ -322,6 +322,58 @@ class DeviceGraph:
             bound = (qd.abs() * torch.maximum(lo_t.abs(), hi_t.abs())).sum(dim=1).max()
         return _lib.DIST_EXACT_F32 if float(bound) < EXACT_LIMIT else _lib.DIST_F64
 
+    # ------------------------------------------------------------------- single-query path
+    def search_one(self, query: NDArray[np.float32], k: int, ef: int) -> tuple[NDArray[np.int64],
+                                                                              NDArray[np.float64],
+                                                                              NDArray[np.int64]]:
+        """One prepared float32 query (dim,), unfiltered, for latency: preallocated device and
+        pinned host buffers, the arithmetic chosen on the host from the query's own values, one
+        library call (which synchronises once) and asynchronous copies either side. Returns host
+        arrays (ids (k,), distances (k,), counters (2,))."""
+        dev = self.device
+        key = int(k)
+        buf = getattr(self, "_one", None)
+        if buf is None or buf["k"] != key:
+            with torch.cuda.device(dev):
+                buf = {
+                    "k": key,
+                    "q": torch.empty((1, self.dim), dtype=torch.float32, device=dev),
+                    "ef": torch.empty(1, dtype=torch.int32, device=dev),
+                    "ids": torch.empty((1, key), dtype=torch.int64, device=dev),
+                    "dists": torch.empty((1, key), dtype=torch.float64, device=dev),
+                    "ctr": torch.empty((1, 2), dtype=torch.int64, device=dev),
+                    "h_q": torch.empty((1, self.dim), dtype=torch.float32).pin_memory(),
+                    "h_ef": torch.empty(1, dtype=torch.int32).pin_memory(),
+                    "h_ids": torch.empty((1, key), dtype=torch.int64).pin_memory(),
+                    "h_dists": torch.empty((1, key), dtype=torch.float64).pin_memory(),
+                    "h_ctr": torch.empty((1, 2), dtype=torch.int64).pin_memory(),
+                }
+            self._one = buf
+        q = np.asarray(query, dtype=np.float32).reshape(1, self.dim)
+        mode = self.choose_mode(q, False)
+        buf["h_q"].numpy()[:] = q
+        buf["h_ef"].numpy()[0] = max(int(ef), key)
+        stream = torch.cuda.current_stream(dev)
+        with torch.cuda.device(dev):
+            buf["q"].copy_(buf["h_q"], non_blocking=True)
+            buf["ef"].copy_(buf["h_ef"], non_blocking=True)
+            args = _lib.SearchArgs(
+                queries=buf["q"].data_ptr(), queries_f64=0, use_codes=0, nq=1, k=key, k_search=key,
+                ef=buf["ef"].data_ptr(), ef_max=max(int(ef), key), dist_mode=int(mode), allowed=None,
+                allowed_fraction=1.0, rerank_queries=None, out_ids=buf["ids"].data_ptr(),
+                out_dists=buf["dists"].data_ptr(), out_counters=buf["ctr"].data_ptr(),
+                stop_mlp=None, stop_threshold=0.0, trace_cap=0, trace_feat=None, trace_dk=None,
+                trace_count=None, trace_hops=None,
+            )
+            _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args),
+                                                 ctypes.c_void_p(stream.cuda_stream)))
+            buf["h_ids"].copy_(buf["ids"], non_blocking=True)
+            buf["h_dists"].copy_(buf["dists"], non_blocking=True)
+            buf["h_ctr"].copy_(buf["ctr"], non_blocking=True)
+            stream.synchronize()
+        return (buf["h_ids"].numpy()[0].copy(), buf["h_dists"].numpy()[0].copy(),
+                buf["h_ctr"].numpy()[0].copy())
+
     # ------------------------------------------------------------------------------ search
     def search(
         self,

@@ -296,6 +296,10 @@ class HNSWIndex:
         prepared = self._prepare(as_vector(query, "query", dim=self._dim)[None, :])
         if allowed is not None and not allowed.any():
             return np.full(k_valid, -1, dtype=np.int64), np.full(k_valid, np.inf)
+        if allowed is None and np.isscalar(ef_valid):  # the latency path
+            ids, dists, ctr = self.device_graph.search_one(prepared[0], k_valid, int(ef_valid))
+            self._counters += ctr
+            return ids, dists
         ids, dists = self._run(prepared, k_valid, ef_valid, allowed)
         return ids[0], dists[0]
 
