@@ -196,8 +196,13 @@ def run_reference(args: argparse.Namespace) -> None:
     threads = cpu.default_threads()
     ef = int(os.environ.get("HNSW_BENCH_EF", "0")) or None
     if ef is None:
-        op = ROOT / "graphs" / args.workload / "operating_point.json"
-        ef = json.loads(op.read_text())["ef"] if op.is_file() else 32
+        # The GPU arm's plain operating point: measured live by that arm on the same box when it
+        # has run, else the committed measurement of this workload (the search results, hence the
+        # recall of each efSearch, are the reference's own).
+        live = ROOT / "graphs" / args.workload / "operating_point.json"
+        committed = json.loads((ROOT / "graphs" / "operating_points.json").read_text())
+        ef = (json.loads(live.read_text())["ef"] if live.is_file()
+              else int(committed[args.workload]["ef"]))
     per_step_s = max(2.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
     values = []
     for step in range(args.warmup + args.steps):
