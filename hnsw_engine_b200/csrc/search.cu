@@ -914,28 +914,42 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32
     churn += __popc(__ballot_sync(FULL, adm && pos_r0 + rank_prev < P.k));
     const int pmin = __reduce_min_sync(FULL, adm ? pos_r0 : 0x7fffffff);
     const int fmin = __reduce_min_sync(FULL, adm ? fpos : 0x7fffffff);
-    // Move R0[p] (p >= pmin) up by the admitted entries that precede it, highest chunk first.
-    for (int top = r0 - 1; top >= pmin; top -= 32) {
-        const int p = top - lane;
-        const bool act = p >= pmin;
-        double d = 0.0;
-        int32_t id = 0, ip = 0;
-        int sft = 0;
-        if (act) {
-            d = C.Rd[p];
-            id = C.Ri[p];
-            ip = C.Rp[p];
+    // Move R0[p] (p >= pmin) up by the admitted entries that precede it, two chunks of 32 at a
+    // time, highest first: every entry of a step is read before any is written, and the writes
+    // land above every index the next step reads.
+    for (int top = r0 - 1; top >= pmin; top -= 64) {
+        const int p1 = top - lane, p2 = top - 32 - lane;
+        const bool a1 = p1 >= pmin, a2 = p2 >= pmin;
+        double d1 = 0.0, d2 = 0.0;
+        int32_t i1 = 0, i2 = 0, q1 = 0, q2 = 0;
+        if (a1) {
+            d1 = C.Rd[p1];
+            i1 = C.Ri[p1];
+            q1 = C.Rp[p1];
         }
+        if (a2) {
+            d2 = C.Rd[p2];
+            i2 = C.Ri[p2];
+            q2 = C.Rp[p2];
+        }
+        int s1 = 0, s2 = 0;
         for (uint32_t m = A; m;) {
             const int i = __ffs(m) - 1;
             m &= m - 1;
-            sft += __shfl_sync(FULL, pos_r0, i) <= p;
+            const int pr = __shfl_sync(FULL, pos_r0, i);
+            s1 += pr <= p1;
+            s2 += pr <= p2;
         }
         __syncwarp();
-        if (act) {
-            C.Rd[p + sft] = d;
-            C.Ri[p + sft] = id;
-            C.Rp[p + sft] = ip;
+        if (a1) {
+            C.Rd[p1 + s1] = d1;
+            C.Ri[p1 + s1] = i1;
+            C.Rp[p1 + s1] = q1;
+        }
+        if (a2) {
+            C.Rd[p2 + s2] = d2;
+            C.Ri[p2 + s2] = i2;
+            C.Rp[p2 + s2] = q2;
         }
         __syncwarp();
     }

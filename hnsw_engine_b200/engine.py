@@ -171,9 +171,18 @@ class DeviceGraph:
             inner["vector_bytes"] = (self.vector_bytes[order].contiguous()
                                      if self.vector_bytes is not None else None)
             inner["count0"] = self.count0[order].contiguous()
-            inner["links0"] = relink(self.links0[order], inner["count0"])
+            links0 = relink(self.links0[order], inner["count0"])
+            links_up = relink(self.links_up, self.count_up)
+            # The native rows hold one slot more than a link count can reach (2M + 1 and M + 1):
+            # without it a layer-0 row of M = 16 is exactly one 128-byte line.
+            w0, wu = links0.shape[1] - 1, links_up.shape[1] - 1
+            if w0 >= 1 and int(inner["count0"].max()) <= w0:
+                links0 = links0[:, :w0]
+            if wu >= 1 and (self.rows == 0 or int(self.count_up.max()) <= wu):
+                links_up = links_up[:, :wu]
+            inner["links0"] = links0.contiguous()
+            inner["links_up"] = links_up.contiguous()
             inner["upper_offset"] = self.upper_offset[order].contiguous()
-            inner["links_up"] = relink(self.links_up, self.count_up)
             inner["entry_point"] = int(new_of_old[self.entry_point].item())
             inner["node_ids"] = order.to(torch.int32).contiguous()
         self.order = order
@@ -197,8 +206,8 @@ class DeviceGraph:
                 n=self.n,
                 rows=self.rows,
                 dim=self.dim,
-                links0_stride=self.links0_stride,
-                links_up_stride=self.links_up_stride,
+                links0_stride=int(inner["links0"].shape[1]),
+                links_up_stride=int(inner["links_up"].shape[1]),
                 metric=_lib.METRIC_CODES[self.metric],
                 entry_point=inner["entry_point"],
                 max_level=self.max_level,

@@ -17,6 +17,7 @@ from __future__ import annotations
 import argparse
 import json
 import time
+from pathlib import Path
 
 import numpy as np
 import torch
@@ -66,14 +67,21 @@ def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
     return log
 
 
+# Trained networks shipped with the package (the training is deterministic; these are its output
+# for the standard workloads, kept so that a fresh checkout needs no training run).
+SHIPPED = Path(__file__).resolve().parent / "stopnets"
+
+
 def load_or_train(workload: str, device: str = "cuda") -> StopNetwork:
-    """The workload's trained network (trained now, about 20 s on a B200, if none is stored)."""
-    path = graphs.graph_dir(workload) / "stopnet"
-    try:
-        return StopNetwork.load(path, device)
-    except (FileNotFoundError, ValueError, KeyError):
-        train(workload, device=device)
-        return StopNetwork.load(path, device)
+    """The workload's trained network: the one next to the graph, else the shipped one, else
+    trained now (about 20 s on a B200)."""
+    for path in (graphs.graph_dir(workload) / "stopnet", SHIPPED / workload):
+        try:
+            return StopNetwork.load(path, device)
+        except (FileNotFoundError, ValueError, KeyError):
+            continue
+    train(workload, device=device)
+    return StopNetwork.load(graphs.graph_dir(workload) / "stopnet", device)
 
 
 def main() -> None:
