@@ -187,22 +187,24 @@ __global__ void mlp_predict_kernel(const float *P, const float *X, int n, float 
     }
 }
 
-// Inference layout used by the search kernel: bf16 W1^T [12][64], bf16 W2^T [64][64], bf16 W3 [64],
-// then float32 b1 [64], b2 [64], b3 [1], feature mean [12], feature 1/std [12].
+// Inference layout used by the search kernel: bf16 W1, W2 and W3 in lane pairs, then float32 b1 [64],
+// b2 [64], b3 [1], feature mean [12], feature 1/std [12]. A pair is the weights of hidden units l and
+// l + 32 for one input, (W[l][i], W[l + 32][i]), stored at [i][l]: lane l reads both of its units'
+// weights for input i in one 32-bit load.
 __global__ void mlp_pack_kernel(const float *P, const float *mean, const float *inv_std,
                                 unsigned char *dst) {
     __nv_bfloat16 *w = reinterpret_cast<__nv_bfloat16 *>(dst);
     float *b = reinterpret_cast<float *>(dst + size_t(H * F + H * H + H) * 2);
     for (int t = threadIdx.x; t < H * F; t += blockDim.x) {
-        const int i = t / H, j = t % H;  // W1^T[i][j] = W1[j][i]
+        const int i = t / H, j = (t % H) / 2 + 32 * (t % 2);  // pair [i][l], half -> unit j
         w[t] = __float2bfloat16_rn(P[O_W1 + j * F + i]);
     }
     for (int t = threadIdx.x; t < H * H; t += blockDim.x) {
-        const int i = t / H, j = t % H;
+        const int i = t / H, j = (t % H) / 2 + 32 * (t % 2);
         w[H * F + t] = __float2bfloat16_rn(P[O_W2 + j * H + i]);
     }
     for (int t = threadIdx.x; t < H; t += blockDim.x) {
-        w[H * F + H * H + t] = __float2bfloat16_rn(P[O_W3 + t]);
+        w[H * F + H * H + t] = __float2bfloat16_rn(P[O_W3 + t / 2 + 32 * (t % 2)]);
         b[t] = P[O_B1 + t];
         b[H + t] = P[O_B2 + t];
     }

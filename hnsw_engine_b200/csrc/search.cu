@@ -169,9 +169,10 @@ struct SearchParams {
 constexpr int STOP_EVERY = 16;
 constexpr int STOP_FEATURES = 12;
 constexpr int STOP_HIDDEN = 64;
-// Packed network in device memory: bf16 W1^T (12 x 64), bf16 W2^T (64 x 64), bf16 W3 (64), then
-// float32 b1 (64), b2 (64), b3 (1), feature mean (12), feature 1/std (12). Transposed so lane j
-// reads column j without bank conflicts; features are standardised in the kernel.
+// Packed network in device memory: bf16 W1 (12 x 32 pairs), W2 (64 x 32 pairs), W3 (32 pairs), then
+// float32 b1 (64), b2 (64), b3 (1), feature mean (12), feature 1/std (12). Pair [i][l] holds the
+// weights of hidden units l and l + 32 for input i, so lane l reads both in one 32-bit load
+// without bank conflicts; features are standardised in the kernel.
 constexpr int MLP_W1 = STOP_FEATURES * STOP_HIDDEN;
 constexpr int MLP_W2 = STOP_HIDDEN * STOP_HIDDEN;
 constexpr int MLP_W3 = STOP_HIDDEN;
@@ -755,35 +756,40 @@ __device__ __forceinline__ int32_t first_link(const int32_t *nb, int stride, int
 // holds the same (uniform) features; lane j computes hidden units j and j + 32.
 __device__ __forceinline__ float mlp_eval(const Ctx &C, const float (&raw)[STOP_FEATURES]) {
     const int lane = C.lane;
-    const __nv_bfloat16 *w1t = C.mlp_w;             // [i][j]
-    const __nv_bfloat16 *w2t = w1t + MLP_W1;        // [i][j]
-    const __nv_bfloat16 *w3 = w2t + MLP_W2;
+    const __nv_bfloat162 *w1 = reinterpret_cast<const __nv_bfloat162 *>(C.mlp_w);  // [i][l]
+    const __nv_bfloat162 *w2 = w1 + STOP_FEATURES * 32;                              // [i][l]
+    const __nv_bfloat162 *w3 = w2 + STOP_HIDDEN * 32;                                // [l]
     const float *b1 = C.mlp_b, *b2 = b1 + STOP_HIDDEN, *b3 = b2 + STOP_HIDDEN;
     const float *mu = b3 + 1, *inv_sd = mu + STOP_FEATURES;
     float f[STOP_FEATURES];
 #pragma unroll
     for (int i = 0; i < STOP_FEATURES; i++) f[i] = (raw[i] - mu[i]) * inv_sd[i];
+    // lane l computes hidden units l (a) and l + 32 (b)
     float ha = b1[lane], hb = b1[lane + 32];
 #pragma unroll
     for (int i = 0; i < STOP_FEATURES; i++) {
-        ha = fmaf(__bfloat162float(w1t[i * STOP_HIDDEN + lane]), f[i], ha);
-        hb = fmaf(__bfloat162float(w1t[i * STOP_HIDDEN + lane + 32]), f[i], hb);
+        const float2 w = __bfloat1622float2(w1[i * 32 + lane]);
+        ha = fmaf(w.x, f[i], ha);
+        hb = fmaf(w.y, f[i], hb);
     }
     ha = fmaxf(ha, 0.f);
     hb = fmaxf(hb, 0.f);
     float ga = b2[lane], gb = b2[lane + 32];
 #pragma unroll 8
     for (int i = 0; i < 32; i++) {
-        const float x = __shfl_sync(FULL, ha, i);
-        const float y = __shfl_sync(FULL, hb, i);
-        ga = fmaf(__bfloat162float(w2t[i * STOP_HIDDEN + lane]), x, ga);
-        gb = fmaf(__bfloat162float(w2t[i * STOP_HIDDEN + lane + 32]), x, gb);
-        ga = fmaf(__bfloat162float(w2t[(i + 32) * STOP_HIDDEN + lane]), y, ga);
-        gb = fmaf(__bfloat162float(w2t[(i + 32) * STOP_HIDDEN + lane + 32]), y, gb);
+        const float x = __shfl_sync(FULL, ha, i);  // hidden unit i
+        const float y = __shfl_sync(FULL, hb, i);  // hidden unit i + 32
+        const float2 wx = __bfloat1622float2(w2[i * 32 + lane]);
+        const float2 wy = __bfloat1622float2(w2[(i + 32) * 32 + lane]);
+        ga = fmaf(wx.x, x, ga);
+        gb = fmaf(wx.y, x, gb);
+        ga = fmaf(wy.x, y, ga);
+        gb = fmaf(wy.y, y, gb);
     }
     ga = fmaxf(ga, 0.f);
     gb = fmaxf(gb, 0.f);
-    float o = __bfloat162float(w3[lane]) * ga + __bfloat162float(w3[lane + 32]) * gb;
+    const float2 w = __bfloat1622float2(w3[lane]);
+    float o = w.x * ga + w.y * gb;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) o += __shfl_xor_sync(FULL, o, off);
     return o + b3[0];
