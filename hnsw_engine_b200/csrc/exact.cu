@@ -347,13 +347,28 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
                 const int valid = min(32, p.row_end - col0);  // columns that are data rows
                 uint32_t keep = 0;
+                // One loop per metric (the branch is uniform): l2 |q|^2 + |x|^2 - 2 q.x; ip -q.x;
+                // cosine 1 - q.x (normalised rows). Columns past the data rows are masked once.
+                if (l2) {
 #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    // l2: |q|^2 + |x|^2 - 2 q.x; ip: -q.x; cosine: 1 - q.x (normalised rows)
-                    const float a = l2 ? fmaf(-2.f, v[j], qq + xv[j]) : (cosine ? 1.f - v[j] : -v[j]);
-                    v[j] = a;
-                    keep |= (a <= thr && j < valid) ? (1u << j) : 0u;
+                    for (int j = 0; j < 32; j++) {
+                        v[j] = fmaf(-2.f, v[j], qq + xv[j]);
+                        keep |= v[j] <= thr ? (1u << j) : 0u;
+                    }
+                } else if (cosine) {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        v[j] = 1.f - v[j];
+                        keep |= v[j] <= thr ? (1u << j) : 0u;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        v[j] = -v[j];
+                        keep |= v[j] <= thr ? (1u << j) : 0u;
+                    }
                 }
+                if (valid < 32) keep &= valid <= 0 ? 0u : (0xffffffffu >> (32 - valid));
                 if (keep && qvalid) {
                     const int cnt = __popc(keep);
                     int o = atomicAdd(p.cand_cnt + q, cnt);
