@@ -70,6 +70,7 @@ struct FilterParams {
     int32_t *cand_id;      // (nq, cap) row ids
     int32_t *cand_cnt;     // (nq,) appended counts (may exceed cap: overflow)
     int32_t cap;
+    int32_t block_min;     // 1: append only the minimum of each 32-row block (the threshold pass)
     int32_t *err;          // nonzero: a bounded wait expired
 };
 
@@ -369,7 +370,22 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                     }
                 }
                 if (valid < 32) keep &= valid <= 0 ? 0u : (0xffffffffu >> (32 - valid));
-                if (keep && qvalid) {
+                if (p.block_min) {
+                    // Threshold pass: the k-th smallest of the blocks' minima is at least the k-th
+                    // smallest of all the values (a subset's k-th is never below the set's), so
+                    // one candidate per block still bounds the k-th distance from above.
+                    float mn = INFINITY;
+#pragma unroll
+                    for (int j = 0; j < 32; j++)
+                        if ((keep >> j) & 1u) mn = fminf(mn, v[j]);
+                    if (keep && qvalid) {
+                        const int o = atomicAdd(p.cand_cnt + q, 1);
+                        if (o < p.cap) {
+                            cv[o] = mn;
+                            ci[o] = col0;
+                        }
+                    }
+                } else if (keep && qvalid) {
                     const int cnt = __popc(keep);
                     int o = atomicAdd(p.cand_cnt + q, cnt);
 #pragma unroll
@@ -679,7 +695,6 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
     const int64_t n_pad = (n + BN - 1) / BN * BN;
     const int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
     const int64_t q_pad = (QB + BM - 1) / BM * BM;
-    const int qtiles = int(q_pad / BM);
     int sms = 148;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -765,9 +780,11 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
         margins_kernel<<<int((nq + 255) / 256), 256, 0, s>>>(qn, int32_t(nq), xmax, kp, terms, metric, mg);
         XT(cudaGetLastError());
         launches += 2;
-        auto run_filter = [&](int64_t row_end) -> int {
+        // Query tiles of this chunk only (the last chunk may be short), rows split to fill the GPU.
+        const int qt_chunk = int((nq + BM - 1) / BM);
+        auto run_filter = [&](int64_t row_end, bool block_min) -> int {
             const int tiles = int((row_end + BN - 1) / BN);
-            const int want_splits = std::max(1, (4 * sms + qtiles - 1) / qtiles);
+            const int want_splits = std::max(1, (4 * sms + qt_chunk - 1) / qt_chunk);
             const int tps = std::max(1, (tiles + want_splits - 1) / want_splits);
             const int splits = (tiles + tps - 1) / tps;
             FilterParams fp;
@@ -784,19 +801,21 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
             fp.cand_id = ci;
             fp.cand_cnt = cnt;
             fp.cap = int32_t(cap);
+            fp.block_min = block_min ? 1 : 0;
             fp.err = err;
             XT(cudaMemsetAsync(cnt, 0, size_t(nq) * 4, s));
-            knn_filter_kernel<<<dim3(qtiles, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
+            knn_filter_kernel<<<dim3(qt_chunk, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
             XT(cudaGetLastError());
             launches++;
             return 0;
         };
         // Pass one: the prefix rows with no threshold give tau (an upper bound of the k-th).
         XT(cudaMemcpyAsync(th, inf.data(), size_t(nq) * 4, cudaMemcpyHostToDevice, s));
-        if (int rc = run_filter(prefix)) return rc;
+        // One candidate per 32-row block suffices while the prefix has at least k blocks.
+        if (int rc = run_filter(prefix, (prefix + 31) / 32 >= k)) return rc;
         select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nq), k, mg, th, tau);
         // Pass two: every row against tau + margin.
-        if (int rc = run_filter(n)) return rc;
+        if (int rc = run_filter(n, false)) return rc;
         int32_t herr[4];
         XT(cudaMemcpyAsync(hc.data(), cnt, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
         XT(cudaMemcpyAsync(herr, err, 16, cudaMemcpyDeviceToHost, s));
