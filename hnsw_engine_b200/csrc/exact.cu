@@ -45,7 +45,12 @@ constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;
 constexpr int B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int EPI_WARPS = 8;  // two per TMEM lane quarter, each taking half of a tile's columns
+// Epilogue warps: EPI_WARPS / 4 per TMEM lane quarter, taking a tile's 32-column chunks in turn.
+#ifndef HB_EPI_WARPS
+#define HB_EPI_WARPS 12
+#endif
+constexpr int EPI_WARPS = HB_EPI_WARPS;
+constexpr int EPI_PER_QUARTER = EPI_WARPS / 4;
 constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
 constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s
@@ -300,9 +305,9 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
     } else if (warp >= 4) {
         // ---------------------------------------------------------------- epilogue
         // Warp w reads TMEM lanes 32 (w % 4) .. +31 (its hardware lane quarter: one query per
-        // thread) and columns [half * BN/2, half * BN/2 + BN/2) of each accumulator.
+        // thread) and every EPI_PER_QUARTER-th 32-column chunk of each accumulator.
         const int quarter = warp & 3;
-        const int half = (warp - 4) >> 2;
+        const int part = (warp - 4) >> 2;  // 0 .. EPI_PER_QUARTER - 1
         const int row = quarter * 32 + lane;  // TMEM lane = query row of the tile
         const int q = qt * BM + row;
         const bool qvalid = q < p.nq;
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int row0 = p.row_begin + (t0 + lt) * BN;
 #pragma unroll 1
-            for (int c = half * (BN / 2); c < (half + 1) * (BN / 2); c += 32) {
+            for (int c = part * 32; c < BN; c += 32 * EPI_PER_QUARTER) {
                 const int col0 = row0 + c;
                 // |x|^2 of the 32 columns: the same addresses in every lane (broadcast loads),
                 // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + 32
@@ -612,6 +617,17 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
 }
 
 // Error bound of the filter arithmetic and the per-query margins (2 e_q).
+// Largest of n non-negative doubles: their bit patterns order as unsigned integers.
+__global__ void max_norm_kernel(const double *xn, int64_t n, unsigned long long *out) {
+    unsigned long long m = 0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += int64_t(gridDim.x) * blockDim.x)
+        m = max(m, static_cast<unsigned long long>(__double_as_longlong(xn[i])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 __global__ void margins_kernel(const double *qnorm, int32_t nq, double xmax, int kp, int terms,
                                int metric, float *margin) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -726,6 +742,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
     const size_t o_cv = carve(size_t(QB) * cap * 4);
     const size_t o_ci = carve(size_t(QB) * cap * 4);
     const size_t o_err = carve(16);
+    const size_t o_mx = carve(16);
     if (int rc = buf.get(off)) return rc;
     char *B = static_cast<char *>(buf.p);
     auto *xb = reinterpret_cast<__nv_bfloat16 *>(B + o_xb);
@@ -749,13 +766,17 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
         X, n, dim, n_pad, kp, terms, 0, cos, xb, xn, xx);
     XT(cudaGetLastError());
     launches++;
-    double xmax = 1.0;  // largest data norm (margins); one host copy per call
+    double xmax = 1.0;  // largest data norm (margins): a device reduction, one 8-byte copy
     if (!cos) {
-        std::vector<double> hn(static_cast<size_t>(n));
-        XT(cudaMemcpyAsync(hn.data(), xn, size_t(n) * 8, cudaMemcpyDeviceToHost, s));
+        auto *mx = reinterpret_cast<unsigned long long *>(B + o_mx);
+        XT(cudaMemsetAsync(mx, 0, 8, s));
+        max_norm_kernel<<<int(std::min<int64_t>(1024, (n + 255) / 256)), 256, 0, s>>>(xn, n, mx);
+        XT(cudaGetLastError());
+        unsigned long long bits = 0;
+        XT(cudaMemcpyAsync(&bits, mx, 8, cudaMemcpyDeviceToHost, s));
         XT(cudaStreamSynchronize(s));
-        xmax = 0.0;
-        for (double v : hn) xmax = std::max(xmax, v);
+        std::memcpy(&xmax, &bits, 8);
+        launches++;
     }
     CUtensorMap tmA, tmB;
     if (int rc = make_map(&tmA, qb, q_pad, kp, BM)) return rc;
