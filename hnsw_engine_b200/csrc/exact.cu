@@ -103,14 +103,17 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// One bounded probe of a barrier phase. The thread may be suspended by the hardware for up to
+// MBAR_SUSPEND_NS while the phase is incomplete (instead of spinning on issue slots).
+constexpr uint32_t MBAR_SUSPEND_NS = 100000;  // 0.1 ms
 __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(MBAR_SUSPEND_NS)
         : "memory");
     return ok != 0;
 }
