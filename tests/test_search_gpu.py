@@ -197,6 +197,22 @@ def test_large_graph_codes_cosine_match_oracle() -> None:
     _oracle_compare(arrays, ep, ml, metric, q, 10, 128, codes=codes)
 
 
+def test_large_graph_codes_in_cell_order_match_oracle() -> None:
+    """Byte codes on the cell-ordered 100K graph (codes permuted with the rows, internal ids in
+    the links, original ids in results and ties), with and without a filter."""
+    from hnsw_engine_b200 import graphs, synthetic
+    from hnsw_engine_b200.quantization import ScalarQuantizer
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload("mix100k")
+    quant = ScalarQuantizer.fit(arrays["vectors"])
+    codes = quant.encode(arrays["vectors"])
+    q = quant.transform_queries(prepare(graphs.workload_queries("mix100k", nq=200), metric), metric)
+    _oracle_compare(arrays, ep, ml, metric, q, 10, 96, codes=codes)
+    mask = synthetic.bernoulli_mask(arrays["vectors"].shape[0], 0.3)
+    _oracle_compare(arrays, ep, ml, metric, q[:64], 10, 48, mask=mask, codes=codes)
+
+
 @pytest.mark.parametrize("name", ["mix1m", "t1m"])
 def test_million_node_graphs_match_oracle(name: str) -> None:
     """The 1M-node workloads (integer L2 and float cosine): ids, distances and counters equal the
