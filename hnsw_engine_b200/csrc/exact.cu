@@ -183,6 +183,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// Two float32 lanes per instruction (Blackwell packed f32x2): each half is rounded exactly as the
+// scalar add / fma, so the results are those of fmaf(-2, v, qq + x) element by element.
+__device__ __forceinline__ void fma_l2_pair(float &v0, float &v1, float qq, float x0, float x1) {
+    asm("{\n\t.reg .b64 rq, rx, rs, rv, rm;\n\t"
+        "mov.b64 rq, {%2, %2};\n\tmov.b64 rx, {%3, %4};\n\t"
+        "add.rn.f32x2 rs, rq, rx;\n\t"
+        "mov.b64 rv, {%0, %1};\n\tmov.b64 rm, {%5, %5};\n\t"
+        "fma.rn.f32x2 rv, rm, rv, rs;\n\tmov.b64 {%0, %1}, rv;\n\t}"
+        : "+f"(v0), "+f"(v1)
+        : "f"(qq), "f"(x0), "f"(x1), "f"(-2.f));
+}
+
 __global__ void __launch_bounds__(FILTER_THREADS, 1)
     knn_filter_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const FilterParams p) {
@@ -360,9 +372,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 // cosine 1 - q.x (normalised rows). Columns past the data rows are masked once.
                 if (l2) {
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        v[j] = fmaf(-2.f, v[j], qq + xv[j]);
+                    for (int j = 0; j < 32; j += 2) {
+                        fma_l2_pair(v[j], v[j + 1], qq, xv[j], xv[j + 1]);
                         keep |= v[j] <= thr ? (1u << j) : 0u;
+                        keep |= v[j + 1] <= thr ? (2u << j) : 0u;
                     }
                 } else if (cosine) {
 #pragma unroll
