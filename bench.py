@@ -289,6 +289,19 @@ def main() -> None:
         if sweep[ef] >= RECALL_TARGET:
             ef_op = ef
             break
+    # The same operating point without the ladder's granularity: the smallest integer efSearch
+    # between the last rung below the target and ef_op (recall rises with ef on these graphs).
+    i_op = EF_LADDER.index(ef_op)
+    lo, hi = (EF_LADDER[i_op - 1] if i_op else k - 1), ef_op
+    ef_fine, rec_fine = ef_op, sweep[ef_op]
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        ids, dists, _ = g.search(q_dev, k, mid, dist_mode=mode)
+        r = recall_of(ids.cpu().numpy(), dists.cpu().numpy(), gt_ids, gt_d, k)
+        if r >= RECALL_TARGET:
+            hi, ef_fine, rec_fine = mid, mid, r
+        else:
+            lo = mid
     if rank == 0:
         try:
             (ROOT / "graphs" / args.workload / "operating_point.json").write_text(
@@ -312,10 +325,14 @@ def main() -> None:
     c_p = torch.empty_like(c_o)
 
     def step_learned():
-        g.search(q_dev, k, cap, out=(ids_o, d_o, c_o), dist_mode=mode, stop=(packed, thr))
+        g.search(q_dev, k, cap, out=(ids_o, d_o, c_o), dist_mode=mode,
+                 stop=(packed, thr, net.slope, net.slope_from))
 
     def step_plain():
         g.search(q_dev, k, ef_op, out=(ids_p, d_p, c_p), dist_mode=mode)
+
+    def step_fine():
+        g.search(q_dev, k, ef_fine, out=(ids_p, d_p, c_p), dist_mode=mode)
 
     for _ in range(max(3, args.warmup)):
         step_learned()
@@ -331,9 +348,11 @@ def main() -> None:
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         ms_learned = timed_steps(step_learned, args.steps, stream)
+        ms_fine = timed_steps(step_fine, args.steps, stream)
         ms_plain = timed_steps(step_plain, args.steps, stream)
     total_l = max_over_ranks(pg, float(sum(ms_learned)), dev)
     total_p = max_over_ranks(pg, float(sum(ms_plain)), dev)
+    fine_qps = job_throughput(world, nq, args.steps, max_over_ranks(pg, float(sum(ms_fine)), dev))
     value = job_throughput(world, nq, args.steps, total_l)
     plain_qps = job_throughput(world, nq, args.steps, total_p)
     mean_ms = total_l / args.steps
@@ -395,12 +414,15 @@ def main() -> None:
                 "method": "learned stop (value) vs plain fixed-ef, equal recall target "
                           f"{RECALL_TARGET}",
                 "learned_stop": {"ef_cap": cap, "threshold": thr, "recall_at_10": rec_l,
+                                 "threshold_slope": net.slope, "slope_from_hops": net.slope_from,
                                  "qps": value, "mean_hops": hops_l,
                                  "validation_threshold": val_threshold},
                 "plain_fixed_ef": {"ef": ef_op, "recall_at_10": rec_p, "qps": plain_qps,
                                    "mean_hops": hops_p,
                                    "achieved_gbs": alg_bytes_plain / (total_p / args.steps / 1000.0) / 1e9},
                 "learned_over_plain": value / plain_qps,
+                "plain_fixed_ef_fine": {"ef": ef_fine, "recall_at_10": rec_fine, "qps": fine_qps},
+                "learned_over_plain_fine": value / fine_qps,
                 "ef_sweep": {str(e): r for e, r in sweep.items()},
                 "l2_policy": "inputs larger than L2 (vectors %d MB + links %d MB > 126 MB)"
                              % (arrays["vectors"].nbytes >> 20, np.asarray(arrays["links0"]).nbytes >> 20),

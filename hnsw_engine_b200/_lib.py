@@ -72,6 +72,8 @@ class SearchArgs(ctypes.Structure):
         ("trace_dk", ctypes.c_void_p),
         ("trace_count", ctypes.c_void_p),
         ("trace_hops", ctypes.c_void_p),
+        ("stop_slope", ctypes.c_float),
+        ("stop_slope_from", ctypes.c_int32),
     ]
 
 

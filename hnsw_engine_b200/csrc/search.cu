@@ -156,7 +156,9 @@ struct SearchParams {
     int32_t s_cap;
     // learned early termination (layer 0, unfiltered): features every STOP_EVERY expansions
     const void *stop_mlp;   // packed network (see mlp_smem_bytes), or NULL
-    float stop_threshold;   // stop once the predicted further recall@k hits fall below it
+    float stop_threshold;   // stop once the predicted further recall@k hits fall below it,
+    float stop_slope;       // plus stop_slope per 64 layer-0 expansions beyond stop_slope_from
+    int32_t stop_slope_from;
     float *trace_feat;      // (n_queries, trace_cap, STOP_FEATURES) or NULL
     double *trace_dk;       // (n_queries, trace_cap, trace_k): first results' distances per checkpoint
     int32_t *trace_count;   // (n_queries,) checkpoints recorded
@@ -852,7 +854,13 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, S
     S.dk_prev2 = S.dk_prev;
     S.dk_prev = dk;
     S.churn = 0;
-    if (C.mlp_w && r >= P.k) return mlp_eval(C, f) < P.stop_threshold;
+    if (C.mlp_w && r >= P.k) {
+        // The threshold rises with the expansions spent: the batch ends with its longest queries,
+        // whose late expansions add the least recall for their time.
+        const float thr = P.stop_threshold +
+                          P.stop_slope * float(max(0, S.hops0 - P.stop_slope_from)) * (1.f / 64.f);
+        return mlp_eval(C, f) < thr;
+    }
     return false;
 }
 
@@ -1841,6 +1849,8 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.s_cap = s_cap;
     P.stop_mlp = use_mlp ? a->stop_mlp : nullptr;
     P.stop_threshold = a->stop_threshold;
+    P.stop_slope = a->stop_slope;
+    P.stop_slope_from = a->stop_slope_from;
     P.trace_feat = filt ? nullptr : a->trace_feat;
     P.trace_dk = a->trace_dk;
     P.trace_count = a->trace_count;
@@ -2091,6 +2101,8 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     P.s_cap = 256;
     P.stop_mlp = use_mlp ? a->stop_mlp : nullptr;
     P.stop_threshold = a->stop_threshold;
+    P.stop_slope = a->stop_slope;
+    P.stop_slope_from = a->stop_slope_from;
     P.trace_feat = a->trace_feat;
     P.trace_dk = a->trace_dk;
     P.trace_count = a->trace_count;

@@ -408,7 +408,8 @@ class DeviceGraph:
         ``allowed``: bool mask (n,) over original ids, or a device uint32 bitmap over internal
         ids (``pack_mask(internal_mask(mask))``). ``rerank_queries``: float32 prepared
         queries for the fused exact re-rank of the first ``k_search`` beam entries. ``stop``:
-        ``(packed network, threshold)`` for the learned early termination; ``trace``: device
+        ``(packed network, threshold[, slope, slope_from])`` for the learned early termination (the
+        threshold rises by ``slope`` per 64 layer-0 expansions beyond ``slope_from``); ``trace``: device
         buffers ``(features (nq, cap, 12) f32, first 16 result distances (nq, cap, 16) f64,
         count (nq,) i32, hops (nq,) i32)``
         filled with the stop features every 16 layer-0 expansions.
@@ -465,6 +466,8 @@ class DeviceGraph:
                 out_counters=_dev_ptr(ctr),
                 stop_mlp=_dev_ptr(stop[0]) if stop is not None else None,
                 stop_threshold=float(stop[1]) if stop is not None else 0.0,
+                stop_slope=float(stop[2]) if stop is not None and len(stop) > 2 else 0.0,
+                stop_slope_from=int(stop[3]) if stop is not None and len(stop) > 3 else 0,
                 trace_cap=int(trace[0].shape[1]) if trace is not None else 0,
                 trace_feat=_dev_ptr(trace[0]) if trace is not None else None,
                 trace_dk=_dev_ptr(trace[1]) if trace is not None else None,

@@ -381,7 +381,7 @@ class HNSWIndex:
             if packed is None:
                 packed = stop.packed()
                 stop._packed_cache = packed
-            stop_arg = (packed, stop.threshold)
+            stop_arg = (packed, stop.threshold, stop.slope, stop.slope_from)
         ids, dists, ctr = g.search(prepared, k, ef, allowed=allowed, stop=stop_arg)
         self._accumulate(ctr)
         if keep_device:

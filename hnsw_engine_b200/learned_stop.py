@@ -159,6 +159,9 @@ class StopNetwork:
         self.mean = np.zeros(FEATURES, np.float32)
         self.std = np.ones(FEATURES, np.float32)
         self.threshold = 0.0
+        # threshold schedule: + slope per 64 layer-0 expansions beyond slope_from (0: constant)
+        self.slope = 0.0
+        self.slope_from = 0
         self.ef_cap = 256
         self.history: list[float] = []
 
@@ -242,6 +245,7 @@ class StopNetwork:
         np.save(root / "std.npy", self.std)
         (root / "meta.json").write_text(json.dumps({
             "step": self.step, "threshold": self.threshold, "ef_cap": self.ef_cap,
+            "slope": self.slope, "slope_from": self.slope_from,
             "history": self.history, "features": FEATURE_NAMES, "stop_every": STOP_EVERY,
         }, indent=2))
 
@@ -259,14 +263,21 @@ class StopNetwork:
             raise ValueError(f"{root}: network trained on different stop features")
         net.step, net.threshold, net.history = meta["step"], meta["threshold"], meta["history"]
         net.ef_cap = int(meta.get("ef_cap", 256))
+        net.slope = float(meta.get("slope", 0.0))
+        net.slope_from = int(meta.get("slope_from", 0))
         return net
+
+    def stop_args(self, threshold: float | None = None) -> tuple[torch.Tensor, float, float, int]:
+        """The ``stop=`` argument of :meth:`DeviceGraph.search` for this network."""
+        return (self.packed(), self.threshold if threshold is None else float(threshold),
+                self.slope, self.slope_from)
 
 
 # ------------------------------------------------------------------------- threshold and search
 def stopped_search(graph: DeviceGraph, queries: Any, k: int, ef: int, packed: torch.Tensor,
-                   threshold: float, **kw: Any):
+                   threshold: float, slope: float = 0.0, slope_from: int = 0, **kw: Any):
     """One batched search with the learned stop; returns device ``(ids, dists, counters)``."""
-    return graph.search(queries, k, ef, stop=(packed, threshold), **kw)
+    return graph.search(queries, k, ef, stop=(packed, threshold, slope, slope_from), **kw)
 
 
 def recall_of(ids: NDArray, dists: NDArray, true_dist: NDArray, k: int) -> float:
@@ -283,7 +294,7 @@ def tune_threshold(graph: DeviceGraph, net: StopNetwork, queries: Any, true_dist
     best = (lo, 0.0)
     for _ in range(iters):
         mid = 0.5 * (lo + hi)
-        ids, d, _ = stopped_search(graph, queries, k, ef, packed, mid)
+        ids, d, _ = stopped_search(graph, queries, k, ef, packed, mid, net.slope, net.slope_from)
         rec = recall_of(ids.cpu().numpy(), d.cpu().numpy(), true_dist, k)
         if rec >= target:
             best = (mid, rec)
@@ -291,7 +302,7 @@ def tune_threshold(graph: DeviceGraph, net: StopNetwork, queries: Any, true_dist
         else:
             hi = mid
     if best[1] == 0.0:
-        ids, d, _ = stopped_search(graph, queries, k, ef, packed, lo)
+        ids, d, _ = stopped_search(graph, queries, k, ef, packed, lo, net.slope, net.slope_from)
         best = (lo, recall_of(ids.cpu().numpy(), d.cpu().numpy(), true_dist, k))
     net.threshold = best[0]
     return best
@@ -308,7 +319,7 @@ def audited_search(graph: DeviceGraph, queries: Any, k: int, ef_cap: int, net: S
     from .exact_knn import exact_search
 
     ids, dists, _ = stopped_search(graph, queries, k, ef_cap, net.packed(), net.threshold,
-                                   counters=False)
+                                   net.slope, net.slope_from, counters=False)
     nq = int(queries.shape[0])
     rng = np.random.default_rng(seed)
     sample = np.sort(rng.choice(nq, size=max(1, int(round(audit_fraction * nq))), replace=False))

@@ -7,7 +7,13 @@
 2. the tensor-core exact k-NN gives each query's exact k-th distance; each checkpoint is labelled
    with the recall@10 hits the search would still gain by running to the cap;
 3. the network is trained with the library's CUDA forward/backward/Adam kernels;
-4. the stop threshold is tuned on 10,000 validation queries (seed 9) for recall@10 >= 0.95.
+4. the stop threshold is tuned on 10,000 validation queries (seed 9) for recall@10 >= 0.95, with
+   the threshold rising by ``STOP_SLOPE`` per 64 layer-0 expansions beyond ``STOP_SLOPE_FROM``
+   (long searches stop more readily; the batch's makespan is set by its longest queries).
+
+    python -m hnsw_engine_b200.train_stop --workload mix1m --retune
+
+re-tunes the threshold of the stored network for the current schedule without retraining.
 
 The model is written to ``graphs/<workload>/stopnet/`` (git-ignored, next to the graph).
 """
@@ -29,6 +35,18 @@ from .learned_stop import StopNetwork, collect_traces, label_traces, tune_thresh
 from .validation import prepare
 
 VALIDATION_SEED = 9
+# Threshold schedule of the trained networks: measured on mix1m at cap 192 and recall 0.95, a slope
+# of 3.2 from 192 expansions cut the batch time 4.35 -> 4.01 ms against a constant threshold
+# (slopes 0.8 to 6.4 from 192 or 256 all land within 1.5% of it; from 128 misses the target).
+STOP_SLOPE = 3.2
+STOP_SLOPE_FROM = 192
+
+
+def _validation(workload: str, index: HNSWIndex, metric: str, k: int, n_val: int):
+    q_val = prepare(graphs.workload_queries(workload, nq=n_val, seed=VALIDATION_SEED), metric)
+    g = index.device_graph
+    _, val_d = exact_search(g.vectors, torch.from_numpy(q_val).to(g.device), k, metric)
+    return q_val, val_d.cpu().numpy()
 
 
 def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
@@ -42,7 +60,6 @@ def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
     g = index.device_graph
     gen_seed = synthetic.TRAIN_SEED if graphs.WORKLOADS[workload]["gen"] == "mixture" else synthetic.T_TRAIN_SEED
     q_train = prepare(graphs.workload_queries(workload, nq=n_train, seed=gen_seed), metric)
-    q_val = prepare(graphs.workload_queries(workload, nq=n_val, seed=VALIDATION_SEED), metric)
     log = {"workload": workload, "n_train": n_train, "ef_cap": ef_cap, "k": k, "target": target}
 
     tr = collect_traces(g, q_train, k, ef_cap)
@@ -55,12 +72,14 @@ def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
 
     net = StopNetwork(g.device)
     net.ef_cap = ef_cap
+    net.slope, net.slope_from = STOP_SLOPE, STOP_SLOPE_FROM
     losses = net.fit(X, y, epochs=epochs)
     log["epoch_losses"] = losses
 
-    _, val_d = exact_search(g.vectors, torch.from_numpy(q_val).to(g.device), k, metric)
-    thr, rec = tune_threshold(g, net, q_val, val_d.cpu().numpy(), k, ef_cap, target)
-    log.update(threshold=thr, validation_recall=rec, seconds=time.time() - t0)
+    q_val, val_d = _validation(workload, index, metric, k, n_val)
+    thr, rec = tune_threshold(g, net, q_val, val_d, k, ef_cap, target)
+    log.update(threshold=thr, slope=net.slope, slope_from=net.slope_from, validation_recall=rec,
+               seconds=time.time() - t0)
     out = graphs.graph_dir(workload) / "stopnet"
     net.save(out)
     (out / "train_log.json").write_text(json.dumps(log, indent=2))
@@ -84,13 +103,36 @@ def load_or_train(workload: str, device: str = "cuda") -> StopNetwork:
     return StopNetwork.load(graphs.graph_dir(workload) / "stopnet", device)
 
 
+def retune(workload: str, path: Path | None = None, k: int = 10, target: float = 0.95,
+           n_val: int = 10_000, device: str = "cuda") -> dict:
+    """Re-tune the stored network's threshold for the current schedule on the validation queries
+    and write it back (to ``path``, default the shipped copy)."""
+    path = SHIPPED / workload if path is None else Path(path)
+    net = StopNetwork.load(path, device)
+    meta, arrays = graphs.open_workload(workload)
+    params = {kk: v for kk, v in meta["params"].items() if kk != "engine"}
+    index = HNSWIndex.from_arrays(arrays, int(meta["entry_point"]), int(meta["max_level"]),
+                                  device=device, **params)
+    q_val, val_d = _validation(workload, index, params["metric"], k, n_val)
+    net.slope, net.slope_from = STOP_SLOPE, STOP_SLOPE_FROM
+    thr, rec = tune_threshold(index.device_graph, net, q_val, val_d, k, net.ef_cap, target)
+    net.save(path)
+    return {"workload": workload, "threshold": thr, "slope": net.slope,
+            "slope_from": net.slope_from, "validation_recall": rec}
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
     p.add_argument("--workload", default="mix1m")
     p.add_argument("--n-train", type=int, default=200_000)
     p.add_argument("--ef-cap", type=int, default=192)
     p.add_argument("--epochs", type=int, default=4)
+    p.add_argument("--retune", action="store_true",
+                   help="only re-tune the shipped network's threshold for the current schedule")
     args = p.parse_args()
+    if args.retune:
+        print(json.dumps(retune(args.workload)), flush=True)
+        return
     print(json.dumps(train(args.workload, args.n_train, args.ef_cap, epochs=args.epochs)), flush=True)
 
 

@@ -114,6 +114,10 @@ typedef struct hnsw_b200_search_args {
                                      checkpoint (+inf beyond the results held) */
     int32_t *trace_count;         /* (nq,) checkpoints recorded */
     int32_t *trace_hops;          /* (nq,) layer-0 expansions of the whole search */
+    /* The stop threshold rises by stop_slope per 64 layer-0 expansions beyond stop_slope_from
+     * (0 and any: a constant threshold). */
+    float stop_slope;
+    int32_t stop_slope_from;
 } hnsw_b200_search_args_t;
 
 #define HNSW_B200_STOP_EVERY 16

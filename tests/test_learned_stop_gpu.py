@@ -83,9 +83,11 @@ def _graph():
     return HNSWIndex.from_arrays(arrays, int(meta["entry_point"]), int(meta["max_level"]), **params).device_graph, name
 
 
-def test_in_kernel_inference_stops_where_the_network_says() -> None:
+@pytest.mark.parametrize("slope,slope_from", [(0.0, 0), (3.2, 32)])
+def test_in_kernel_inference_stops_where_the_network_says(slope: float, slope_from: int) -> None:
     """A stopped search ends at the first checkpoint whose host-side prediction is below the
-    threshold (the trajectory up to there is the plain search's)."""
+    threshold schedule, thr + slope * max(0, hops - slope_from) / 64 (the trajectory up to there is
+    the plain search's)."""
     from hnsw_engine_b200 import graphs
     from hnsw_engine_b200.learned_stop import collect_traces
 
@@ -104,16 +106,19 @@ def test_in_kernel_inference_stops_where_the_network_says() -> None:
     td = torch.empty((m, 64, 16), dtype=torch.float64, device="cuda")
     tc = torch.zeros(m, dtype=torch.int32, device="cuda")
     th = torch.zeros(m, dtype=torch.int32, device="cuda")
-    g.search(q, 10, 256, stop=(net.packed(), thr), trace=(tf, td, tc, th))
+    g.search(q, 10, 256, stop=(net.packed(), thr, slope, slope_from), trace=(tf, td, tc, th))
     stop_hops = th.cpu().numpy()
+    hops = 16 * np.arange(1, pred.shape[1] + 1)
+    sched = (thr + np.float32(slope) * np.maximum(0, hops - slope_from).astype(np.float32)
+             * np.float32(1 / 64)).astype(np.float32)
     checked = 0
     for i in range(m):
         c = tr.count[i]
-        below = np.flatnonzero(pred[i, :c] < thr)
-        if below.size and np.all(np.abs(pred[i, : below[0] + 1] - thr) > 1e-4):
+        below = np.flatnonzero(pred[i, :c] < sched[:c])
+        if below.size and np.all(np.abs(pred[i, : below[0] + 1] - sched[: below[0] + 1]) > 1e-4):
             assert stop_hops[i] == 16 * (below[0] + 1), i
             checked += 1
-        elif not below.size and np.all(np.abs(pred[i, :c] - thr) > 1e-4):
+        elif not below.size and np.all(np.abs(pred[i, :c] - sched[:c]) > 1e-4):
             assert stop_hops[i] == tr.hops[i], i
             checked += 1
     assert checked > 0.9 * m
