@@ -170,12 +170,18 @@ def cpu_sample(arrays, ep, ml, queries, k, ef, metric, seconds: float, threads: 
     t0 = time.perf_counter()
     cpu.search_batch(arrays, ep, ml, queries[:probe], k, ef, metric, threads=threads)
     per_q = (time.perf_counter() - t0) / probe
-    n = int(min(len(queries), max(probe, seconds / max(per_q, 1e-9))))
+    # about `seconds` of work: the workload's queries, cycled when one pass takes less
+    n = int(min(16 * len(queries), max(probe, seconds / max(per_q, 1e-9))))
+    sample = queries[np.arange(n) % len(queries)]
+    if not np.isscalar(ef):
+        ef = np.asarray(ef)[np.arange(n) % len(queries)]
     t0 = time.perf_counter()
-    cpu.search_batch(arrays, ep, ml, queries[:n], k, ef, metric, threads=threads)
+    cpu.search_batch(arrays, ep, ml, sample, k, ef, metric, threads=threads)
     el = time.perf_counter() - t0
     return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} of {len(queries)} queries at ef={ef if np.isscalar(ef) else 'per-query'}, "
+            "sample": f"{n} queries ({len(queries)} workload queries"
+                      f"{', cycled' if n > len(queries) else ''}) at "
+                      f"ef={ef if np.isscalar(ef) else 'per-query'}, "
                       f"C restatement of the reference search (oracle/hnsw_oracle.c), "
                       f"{threads} threads, {el:.1f} s"}
 
