@@ -97,6 +97,17 @@ class ExactArgs(ctypes.Structure):
     ]
 
 
+class ValueStats(ctypes.Structure):
+    """``hnsw_b200_value_stats_t``."""
+
+    _fields_ = [
+        ("finite", ctypes.c_int32),
+        ("integer", ctypes.c_int32),
+        ("min", ctypes.c_double),
+        ("max", ctypes.c_double),
+    ]
+
+
 # Every symbol include/hnsw_b200.h declares, with its ctypes signature.
 SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "hnsw_b200_open": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.POINTER(ctypes.c_void_p)]),
@@ -129,6 +140,9 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                                               ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_validate_graph": (ctypes.c_int, [ctypes.POINTER(Graph), ctypes.c_void_p, ctypes.c_int32,
                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                                ctypes.c_void_p]),
+    "hnsw_b200_upload_queries": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                ctypes.c_int32, ctypes.POINTER(ValueStats),
                                                 ctypes.c_void_p]),
     "hnsw_b200_version": (ctypes.c_char_p, []),
 }

@@ -13,7 +13,7 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = sorted((PKG / "csrc").glob("*.cu"))
+SOURCES = sorted((PKG / "csrc").glob("*.cu")) + sorted((PKG / "csrc").glob("*.cpp"))  # .cpp: host only
 OUT = PKG / "libhnsw_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -34,7 +34,8 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile every ``csrc/*.cu`` into ``libhnsw_b200.so`` (skipped when up to date)."""
+    """Compile every ``csrc/*.cu`` and ``csrc/*.cpp`` into ``libhnsw_b200.so`` (skipped when up to
+    date)."""
     if not force and not needs_build():
         return OUT
     cmd = [

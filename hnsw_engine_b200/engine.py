@@ -24,6 +24,8 @@ from numpy.typing import NDArray
 from . import _lib
 
 EXACT_LIMIT = float(2**24)
+# Host threads that read an uploaded query batch for its statistics (the library's pool size caps it).
+UPLOAD_THREADS = 8
 # Graphs of at least this many nodes with byte rows are stored on the GPU in a locality order (see
 # DeviceGraph._build_internal_order); smaller ones fit in L2 and keep the reference's order.
 LOCALITY_MIN_NODES = 65536
@@ -45,8 +47,11 @@ def pack_mask(mask: NDArray[np.bool_]) -> NDArray[np.uint32]:
 
 
 def to_device(a: Any, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
-    """Host array or device tensor -> contiguous device tensor of ``dtype`` (H2D copy if host)."""
+    """Host array or device tensor -> contiguous device tensor of ``dtype`` (H2D copy if host; an
+    asynchronous one on the current stream from a page-locked tensor of that dtype)."""
     if isinstance(a, torch.Tensor):
+        if not a.is_cuda and a.dtype == dtype and a.is_contiguous() and a.is_pinned():
+            return a.to(device=device, non_blocking=True)
         return a.to(device=device, dtype=dtype).contiguous()
     arr = np.ascontiguousarray(a)
     t = torch.from_numpy(arr)
@@ -303,13 +308,42 @@ class DeviceGraph:
             bound = (np.abs(q) * np.maximum(np.abs(lo), np.abs(hi))).sum(axis=1).max()
         return bool(bound < EXACT_LIMIT)
 
+    def upload_queries(self, src: NDArray[np.float32], dst: torch.Tensor | None,
+                       threads: int = UPLOAD_THREADS) -> _lib.ValueStats:
+        """Copy C-contiguous float32 host queries into the device tensor ``dst`` on the current
+        stream (``None``: no copy) and return their statistics (finite, integer, min, max), read
+        on host threads in the library while the copy runs."""
+        st = _lib.ValueStats()
+        if dst is None:
+            _lib.check(self.lib.hnsw_b200_upload_queries(src.ctypes.data, None, src.size,
+                                                          int(threads), ctypes.byref(st), None))
+            return st
+        if dst.numel() != src.size or dst.dtype != torch.float32 or not dst.is_contiguous():
+            raise ValueError("dst must be a contiguous float32 device tensor of src's size")
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(self.lib.hnsw_b200_upload_queries(
+                src.ctypes.data, _dev_ptr(dst), src.size, int(threads), ctypes.byref(st),
+                ctypes.c_void_p(stream)))
+        return st
+
+    def mode_from_stats(self, st: _lib.ValueStats, queries: NDArray[np.float32]) -> int:
+        """:meth:`choose_mode` from :meth:`upload_queries` statistics (uncoded queries): the same
+        rules; only integer data outside the byte range still needs the host's per-row bound."""
+        if queries.size == 0 or self.metric == "cosine" or not st.integer:
+            return _lib.DIST_F64
+        if self.dim % 4 == 0 and self.vector_bytes is not None and st.min >= 0 and st.max <= 255:
+            return _lib.DIST_BYTES
+        return _lib.DIST_EXACT_F32 if self.exact_f32_ok(queries, False) else _lib.DIST_F64
+
     def choose_mode_device(self, q: torch.Tensor, codes: bool) -> int:
         """:meth:`choose_mode` for queries already on this GPU: the same rules, evaluated by a few
         device reductions and one small copy back, instead of a host pass over the batch."""
         if q.numel() == 0:
             return _lib.DIST_F64
-        qd = q.to(torch.float64)
-        st = torch.stack([(qd != torch.round(qd)).any().to(torch.float64), qd.min(), qd.max()]).cpu()
+        # integrality, minimum and maximum in q's own dtype (exact for float32 and float64 alike)
+        lo_q, hi_q = torch.aminmax(q)
+        st = torch.stack([(q != torch.round(q)).any().to(q.dtype), lo_q, hi_q]).to(torch.float64).cpu()
         integer = not bool(st[0])
         if self.metric == "cosine" or not integer:
             return _lib.DIST_F64
@@ -322,6 +356,7 @@ class DeviceGraph:
             lo, hi = self._lo, self._hi
         else:
             return _lib.DIST_F64
+        qd = q.to(torch.float64)
         lo_t = torch.from_numpy(np.asarray(lo, dtype=np.float64)).to(qd.device)
         hi_t = torch.from_numpy(np.asarray(hi, dtype=np.float64)).to(qd.device)
         if self.metric == "l2":
@@ -425,6 +460,9 @@ class DeviceGraph:
             if isinstance(ef, torch.Tensor):
                 ef_t = ef.to(device=dev, dtype=torch.int32).contiguous()
                 ef_max = int(ef_t.max().item()) if nq else 1
+            elif np.ndim(ef) == 0:
+                ef_max = int(ef) if nq else 1
+                ef_t = torch.full((nq,), int(ef), dtype=torch.int32, device=dev)
             else:
                 ef_arr = np.broadcast_to(np.asarray(ef, dtype=np.int32), (nq,))
                 ef_max = int(ef_arr.max()) if nq else 1

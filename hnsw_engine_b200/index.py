@@ -49,6 +49,14 @@ SELECTIONS = ("simple", "heuristic")
 
 
 @dataclass(frozen=True)
+class _Uploaded:
+    """Checked, prepared queries already on the GPU, with their distance arithmetic."""
+
+    rows: torch.Tensor
+    dist_mode: int
+
+
+@dataclass(frozen=True)
 class IndexStats:
     """Summary of an index, with the fields of the reference's ``IndexStats`` (index.py:63-93)."""
 
@@ -146,6 +154,7 @@ class HNSWIndex:
         self._arrays: dict[str, NDArray[Any]] | None = None
         self._size = 0
         self._counters = np.zeros(2, dtype=np.int64)  # distance computations, hops
+        self._counters_dev: torch.Tensor | None = None  # device-side share not yet read back
         self._meta_extra: dict[str, Any] = {}
 
     # ----------------------------------------------------------------------- opening
@@ -228,11 +237,18 @@ class HNSWIndex:
 
     @property
     def distance_computations(self) -> int:
-        return int(self._counters[0])
+        return int(self._read_counters()[0])
 
     @property
     def hops(self) -> int:
-        return int(self._counters[1])
+        return int(self._read_counters()[1])
+
+    def _read_counters(self) -> NDArray[np.int64]:
+        """Fold the searches' device-side counter sums into the host totals (one small copy)."""
+        if self._counters_dev is not None:
+            self._counters += self._counters_dev.cpu().numpy()
+            self._counters_dev = None
+        return self._counters
 
     def native_arrays(self) -> dict[str, NDArray[Any]]:
         if self._arrays is None:
@@ -258,6 +274,28 @@ class HNSWIndex:
     # --------------------------------------------------------------------------- search
     def _prepare(self, vectors: ArrayLike) -> NDArray[np.float32]:
         return prepare(as_matrix(vectors, "vectors", dim=self._dim), self._metric)
+
+    def _upload(self, vectors: ArrayLike) -> Any:
+        """Host queries for a device search, with :meth:`_prepare`'s checks, messages and values.
+
+        C-contiguous float32 rows of the right width under l2 or ip are already their prepared
+        form: the library copies them to the GPU while its host threads read them for the NaN/inf
+        check and for the statistics that pick the distance arithmetic, so nothing is read back
+        from the GPU (``_Uploaded``). Every other input is checked and prepared by NumPy, straight
+        into page-locked memory."""
+        a = np.asarray(vectors)
+        if (self._metric != "cosine" and a.dtype == np.float32 and a.ndim == 2
+                and a.shape[1] == self._dim and a.flags.c_contiguous):
+            g = self.device_graph
+            rows = torch.empty(a.shape, dtype=torch.float32, device=g.device)
+            st = g.upload_queries(a, rows)
+            if not st.finite:
+                raise ValueError("vectors contains NaN or infinite values")
+            return _Uploaded(rows, g.mode_from_stats(st, a))
+        rows = as_matrix(a, "vectors", dim=self._dim)
+        staged = torch.empty(rows.shape, dtype=torch.float32, pin_memory=True)
+        prepare(rows, self._metric, out=staged.numpy(), checked_finite=True)
+        return staged
 
     def _check_search_args(self, k: int, ef: Any) -> tuple[int, Any]:
         if len(self) == 0:
@@ -334,8 +372,13 @@ class HNSWIndex:
             if self._metric == "cosine":
                 q64 = queries.to(torch.float64)
                 prepared = (q64 / torch.linalg.norm(q64, dim=1, keepdim=True)).to(torch.float32)
+        elif allowed is not None and not allowed.any():
+            prepared = self._prepare(queries)  # validated; no device work follows
         else:
-            prepared = self._prepare(queries)
+            prepared = self._upload(queries)
+        dist_mode = None
+        if isinstance(prepared, _Uploaded):
+            prepared, dist_mode = prepared.rows, prepared.dist_mode
         nq = prepared.shape[0]
         if allowed is not None and not allowed.any():
             ids = np.full((nq, k_valid), -1, dtype=np.int64)
@@ -346,7 +389,7 @@ class HNSWIndex:
         if allowed is not None and exact_below is not None and allowed.mean() < float(exact_below):
             return self._exact_subset(prepared, k_valid, allowed, keep_device=on_device)
         ids_t, dists_t = self._run(prepared, k_valid, ef_valid, allowed, keep_device=on_device,
-                                   stop=stop)
+                                   stop=stop, dist_mode=dist_mode)
         return ids_t, dists_t
 
     def _exact_subset(self, prepared: Any, k: int, allowed: NDArray[np.bool_],
@@ -373,7 +416,8 @@ class HNSWIndex:
         return ids.cpu().numpy(), dists.cpu().numpy()
 
     def _run(self, prepared: Any, k: int, ef: Any, allowed: NDArray[np.bool_] | None,
-             keep_device: bool = False, stop: Any = None) -> tuple[Any, Any]:
+             keep_device: bool = False, stop: Any = None,
+             dist_mode: int | None = None) -> tuple[Any, Any]:
         g = self.device_graph
         stop_arg = None
         if stop is not None and allowed is None:
@@ -382,15 +426,24 @@ class HNSWIndex:
                 packed = stop.packed()
                 stop._packed_cache = packed
             stop_arg = (packed, stop.threshold, stop.slope, stop.slope_from)
-        ids, dists, ctr = g.search(prepared, k, ef, allowed=allowed, stop=stop_arg)
+        ids, dists, ctr = g.search(prepared, k, ef, allowed=allowed, stop=stop_arg,
+                                   dist_mode=dist_mode)
         self._accumulate(ctr)
         if keep_device:
             return ids, dists
-        return ids.cpu().numpy(), dists.cpu().numpy()
+        # results into page-locked host memory, one synchronisation for both copies
+        ids_h = torch.empty(ids.shape, dtype=ids.dtype, pin_memory=True)
+        dists_h = torch.empty(dists.shape, dtype=dists.dtype, pin_memory=True)
+        ids_h.copy_(ids, non_blocking=True)
+        dists_h.copy_(dists, non_blocking=True)
+        torch.cuda.current_stream(g.device).synchronize()
+        return ids_h.numpy(), dists_h.numpy()
 
     def _accumulate(self, ctr: torch.Tensor | None) -> None:
+        """Add a search's per-query counters to the running totals on the device (no sync)."""
         if ctr is not None and ctr.numel():
-            self._counters += ctr.sum(dim=0).cpu().numpy()
+            s = ctr.sum(dim=0)
+            self._counters_dev = s if self._counters_dev is None else self._counters_dev + s
 
     # ----------------------------------------------------------------------- inspection
     def stats(self) -> IndexStats:
@@ -427,6 +480,7 @@ class HNSWIndex:
 
     def reset_counters(self) -> None:
         self._counters[:] = 0
+        self._counters_dev = None
 
     def _params(self) -> dict[str, Any]:
         return {

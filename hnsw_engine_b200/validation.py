@@ -72,12 +72,28 @@ def check_k(k: object, n: int) -> int:
     return k_int
 
 
-def prepare(vectors: NDArray[Any], metric: str) -> NDArray[np.float32]:
-    """Stored representation of validated rows: contiguous float32 (cosine: float64-normalised)."""
+def _exact_in_float32(dtype: np.dtype) -> bool:
+    """Finite values of this dtype stay finite in float32 (no overflow on the cast)."""
+    return bool(np.issubdtype(dtype, np.integer) or dtype in (np.float16, np.float32))
+
+
+def prepare(vectors: NDArray[Any], metric: str, out: NDArray[np.float32] | None = None,
+            checked_finite: bool = False) -> NDArray[np.float32]:
+    """Stored representation of validated rows: contiguous float32 (cosine: float64-normalised).
+
+    ``out``: a C-contiguous float32 array of the same shape to write into (a pinned staging
+    buffer), else a new array (or ``vectors`` itself when already contiguous float32).
+    ``checked_finite``: the rows already passed :func:`as_matrix`, so the overflow check after a
+    cast that cannot overflow (integers, float16, float32) is skipped."""
     if metric != "cosine":
         with np.errstate(over="ignore"):
-            direct = np.ascontiguousarray(vectors, dtype=np.float32)
-        if not np.isfinite(direct).all():
+            if out is None:
+                direct = np.ascontiguousarray(vectors, dtype=np.float32)
+            else:
+                np.copyto(out, vectors, casting="unsafe")
+                direct = out
+        skip = checked_finite and _exact_in_float32(np.asarray(vectors).dtype)
+        if not skip and not np.isfinite(direct).all():
             raise ValueError("vectors overflow float32 (values beyond about 3.4e38)")
         return direct
     as64 = np.asarray(vectors, dtype=np.float64)
@@ -88,7 +104,10 @@ def prepare(vectors: NDArray[Any], metric: str) -> NDArray[np.float32]:
             f"cosine distance is undefined for zero vectors (rows {zero_rows[:5].tolist()})"
         )
     with np.errstate(over="ignore"):
-        out = np.ascontiguousarray(as64 / norms[:, None], dtype=np.float32)
+        if out is None:
+            out = np.ascontiguousarray(as64 / norms[:, None], dtype=np.float32)
+        else:
+            np.copyto(out, as64 / norms[:, None], casting="unsafe")
     if not np.isfinite(out).all():
         raise ValueError("vectors overflow float32 (values beyond about 3.4e38)")
     return out

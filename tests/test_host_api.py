@@ -101,3 +101,23 @@ def test_prepare_follows_the_reference() -> None:
 def test_add_is_left_to_the_reference_build() -> None:
     with pytest.raises(NotImplementedError):
         _index().add(np.zeros((1, 4), np.float32))
+
+
+@pytest.mark.parametrize("metric", ["l2", "cosine", "ip"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32, np.int16, np.uint8])
+def test_prepare_into_a_staging_buffer_matches(metric, dtype) -> None:
+    # batch_search writes prepared queries straight into page-locked memory: same values
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal((33, 8)) * 50 + 60).astype(dtype)
+    out = np.empty((33, 8), np.float32)
+    got = prepare(x, metric, out=out, checked_finite=True)
+    assert got is out
+    np.testing.assert_array_equal(out, prepare(x, metric))
+
+
+def test_prepare_into_a_buffer_still_reports_overflow() -> None:
+    out = np.empty((1, 2), np.float32)
+    with pytest.raises(ValueError, match="overflow float32"):
+        prepare(np.array([[1e39, 0.0]]), "l2", out=out, checked_finite=True)
+    with pytest.raises(ValueError, match="overflow float32"):
+        prepare(np.array([[np.inf, 0.0]], np.float32), "l2")

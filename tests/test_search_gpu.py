@@ -73,6 +73,12 @@ def test_device_mode_choice_equals_host_choice() -> None:
             dev = torch.from_numpy(np.ascontiguousarray(b, dtype=np.float64 if codes else np.float32)).cuda()
             host = g.choose_mode(b, codes) if b.size else g.choose_mode_device(dev, codes)
             assert g.choose_mode_device(dev, codes) == host
+            if not codes:  # and from the statistics of the upload's host pass
+                src = np.ascontiguousarray(b, dtype=np.float32)
+                dst = torch.empty(src.shape, dtype=torch.float32, device="cuda")
+                st = g.upload_queries(src, dst)
+                assert g.mode_from_stats(st, src) == host
+                assert torch.equal(dst.cpu(), torch.from_numpy(src))
 
 
 def test_per_query_ef_matches_grouped_reference_calls() -> None:
@@ -112,6 +118,29 @@ def test_single_query_search_matches_batch() -> None:
         a, b = index.search(case["queries"][row], k=5, ef=30)
         np.testing.assert_array_equal(a, ids[row])
         np.testing.assert_array_equal(b, dists[row])
+
+
+def test_host_query_forms_agree_and_reject_nan_alike() -> None:
+    """Contiguous float32 host queries are copied to the GPU as they are and checked there; other
+    dtypes and layouts are checked and prepared on the host. Same results, same error."""
+    case = load_golden("search_cont_l2")
+    arrays, ep, ml = case_arrays(case, "cont_l2")
+    index = _index(arrays, ep, ml, "l2", 8)
+    q = np.ascontiguousarray(case["queries"], dtype=np.float32)
+    want = index.batch_search(q, k=10, ef=30)
+    for form in (q.astype(np.float64), np.asfortranarray(q), q.tolist()):
+        for a, b in zip(want, index.batch_search(form, k=10, ef=30), strict=True):
+            np.testing.assert_array_equal(a, b)
+    mask = np.zeros(arrays["vectors"].shape[0], dtype=bool)
+    mask[:5] = True
+    for bad_value in (np.nan, np.inf):
+        bad = q.copy()
+        bad[3, 1] = bad_value
+        for form in (bad, bad.astype(np.float64)):
+            with pytest.raises(ValueError, match="vectors contains NaN or infinite values"):
+                index.batch_search(form, k=10, ef=30)
+            with pytest.raises(ValueError, match="vectors contains NaN or infinite values"):
+                index.batch_search(form, k=10, ef=30, filter=mask, exact_below=0.05)
 
 
 def test_all_false_filter_pads_without_searching() -> None:

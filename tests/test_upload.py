@@ -1,0 +1,73 @@
+"""The host pass of the query upload (``hnsw_b200_upload_queries`` with no device destination, so
+no GPU work): the statistics that choose the distance arithmetic equal NumPy's, for every split of
+the batch over host threads. The copy itself is checked on the GPU through ``batch_search``."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from hnsw_engine_b200 import _lib, build
+
+    build.build()
+    return _lib.load()
+
+
+def _scan(lib, x: np.ndarray, threads: int):
+    from hnsw_engine_b200._lib import ValueStats, check
+
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    st = ValueStats()
+    check(lib.hnsw_b200_upload_queries(x.ctypes.data, None, x.size, threads, ctypes.byref(st), None))
+    return st
+
+
+def _cases():
+    rng = np.random.default_rng(4)
+    n = 3 * 65536 + 7
+    yield "integers", rng.integers(0, 256, n).astype(np.float32)
+    yield "negative integers", rng.integers(-300, 300, n).astype(np.float32)
+    yield "gaussian", rng.standard_normal(n).astype(np.float32)
+    big = rng.integers(0, 256, n).astype(np.float32)
+    big[n // 2] = 1e30  # every float32 beyond 2^23 is an integer
+    yield "huge", big
+    half = rng.integers(0, 256, n).astype(np.float32)
+    half[-1] = 8388607.5  # the largest non-integer float32, in the last part
+    yield "largest fraction", half
+    neg0 = np.zeros(1000, np.float32)
+    neg0[5] = -0.0
+    yield "signed zeros", neg0
+    yield "one value", np.array([3.25], np.float32)
+    yield "empty", np.zeros(0, np.float32)
+    for bad in (np.nan, np.inf, -np.inf):
+        v = rng.integers(0, 256, n).astype(np.float32)
+        v[2 * 65536 + 3] = bad
+        yield f"{bad}", v
+
+
+@pytest.mark.parametrize("threads", [1, 3, 16])
+def test_upload_statistics_match_numpy(lib, threads: int) -> None:
+    for name, x in _cases():
+        st = _scan(lib, x, threads)
+        finite = bool(np.isfinite(x).all())
+        assert st.finite == int(finite), name
+        if finite:
+            assert st.integer == int(np.array_equal(x, np.rint(x))), name
+            if x.size:
+                assert (st.min, st.max) == (float(x.min()), float(x.max())), name
+            else:
+                assert (st.min, st.max) == (0.0, 0.0)
+
+
+def test_upload_rejects_null_arguments(lib) -> None:
+    from hnsw_engine_b200._lib import ValueStats
+
+    st = ValueStats()
+    assert lib.hnsw_b200_upload_queries(None, None, 4, 1, ctypes.byref(st), None) == -1
+    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, None, None) == -1
+    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, ctypes.byref(st), None) == 0
