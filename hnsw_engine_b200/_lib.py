@@ -74,6 +74,7 @@ class SearchArgs(ctypes.Structure):
         ("trace_hops", ctypes.c_void_p),
         ("stop_slope", ctypes.c_float),
         ("stop_slope_from", ctypes.c_int32),
+        ("priority", ctypes.c_void_p),
     ]
 
 

@@ -29,6 +29,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -1553,6 +1555,11 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
     }
 }
 
+// Row numbers 0 .. n-1 (the values sorted by priority into the first work list).
+__global__ void iota_rows(int32_t *out, int32_t n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = i;
+}
+
 // Collect the work items whose status is nonzero into qlist_out (order: by query row).
 __global__ void collect_failed(const int32_t *status, const int32_t *qlist, int32_t n_work,
                                int32_t *out, int32_t *n_out) {
@@ -1610,6 +1617,7 @@ struct Handle {
     Buffer counters;  // queue, n_failed, n_list
     Buffer status;
     Buffer qlist[2];  // retry work lists (ping-pong)
+    Buffer order_rows, order_keys, order_list, sort_temp;  // start order by priority
     Buffer vis, ties, spill_d, spill_i, spill_p, vbits, vlist;
     bool bits_dirty = false;  // a launch failed mid-flight: bitmaps must be re-zeroed
     int32_t *host_pinned = nullptr;  // 4 ints
@@ -1741,6 +1749,10 @@ void hnsw_b200_close(void *handle) {
     h->status.release();
     h->qlist[0].release();
     h->qlist[1].release();
+    h->order_rows.release();
+    h->order_keys.release();
+    h->order_list.release();
+    h->sort_temp.release();
     h->vis.release();
     h->vbits.release();
     h->vlist.release();
@@ -1863,6 +1875,27 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
 
     int32_t n_work = nq;
     const int32_t *qlist = nullptr;
+    if (a->priority && nq > 1) {
+        // First work list: rows by descending priority, stably (CUB radix sort of the low 16 bits
+        // of the keys with the rows as values); always a permutation of the rows.
+        const size_t rb = size_t(nq) * sizeof(int32_t);
+        if (int rc = h.order_rows.ensure(rb)) return rc;
+        if (int rc = h.order_keys.ensure(rb)) return rc;
+        if (int rc = h.order_list.ensure(rb)) return rc;
+        int32_t *rows = static_cast<int32_t *>(h.order_rows.ptr);
+        int32_t *keys = static_cast<int32_t *>(h.order_keys.ptr);
+        int32_t *list = static_cast<int32_t *>(h.order_list.ptr);
+        iota_rows<<<std::max(1, std::min(1024, (nq + 255) / 256)), 256, 0, s>>>(rows, nq);
+        CUDA_TRY(cudaGetLastError());
+        h.launches++;
+        size_t temp = 0;
+        CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, temp, a->priority, keys, rows,
+                                                           list, nq, 0, 16, s));
+        if (int rc = h.sort_temp.ensure(std::max<size_t>(temp, 16))) return rc;
+        CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(h.sort_temp.ptr, temp, a->priority, keys,
+                                                           rows, list, nq, 0, 16, s));
+        qlist = list;
+    }
     for (int attempt = 0; attempt < 6; attempt++) {
         const int blocks = int(std::min<int64_t>(int64_t(h.sms) * bps, (n_work + WPB - 1) / WPB));
         const int64_t slots = int64_t(blocks) * WPB;

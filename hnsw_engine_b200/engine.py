@@ -22,6 +22,7 @@ import torch
 from numpy.typing import NDArray
 
 from . import _lib
+from .schedule import MIN_QUERIES, CellSchedule
 
 EXACT_LIMIT = float(2**24)
 # Host threads that read an uploaded query batch for its statistics (the library's pool size caps it).
@@ -119,6 +120,10 @@ class DeviceGraph:
         self.locality = bool(locality) and self.n > 1
         self.order: torch.Tensor | None = None  # internal node -> original id (None: identity)
         self._order_host: NDArray[np.int64] | None = None
+        # Longest-predicted-first start order of large batches (graphs with cells only); set
+        # False to start queries in row order. Results are the same either way.
+        self.schedule = True
+        self._schedule: CellSchedule | None = None
         self._internal: dict[str, Any] = {}
         if validate_M is not None:  # before anything follows the links
             self._validate_on_device(arrays["levels"], int(validate_M))
@@ -190,6 +195,7 @@ class DeviceGraph:
             inner["upper_offset"] = self.upper_offset[order].contiguous()
             inner["entry_point"] = int(new_of_old[self.entry_point].item())
             inner["node_ids"] = order.to(torch.int32).contiguous()
+            self._schedule = CellSchedule(pivots)
         self.order = order
         self._order_host = order.cpu().numpy()
 
@@ -480,6 +486,14 @@ class DeviceGraph:
             rq = None
             if rerank_queries is not None:
                 rq = to_device(rerank_queries, torch.float32, dev)
+            sched = self._schedule if (self.schedule and self._schedule is not None
+                                       and nq >= MIN_QUERIES and bitmap is None and not use_codes
+                                       and trace is None) else None
+            cells = prio = None
+            stopped = stop is not None
+            if sched is not None:
+                cells = sched.cells(q)
+                prio = sched.priority(cells, ef_t, stopped)
             if out is None:
                 ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
                 dists = torch.empty((nq, k), dtype=torch.float64, device=dev)
@@ -511,7 +525,10 @@ class DeviceGraph:
                 trace_dk=_dev_ptr(trace[1]) if trace is not None else None,
                 trace_count=_dev_ptr(trace[2]) if trace is not None else None,
                 trace_hops=_dev_ptr(trace[3]) if trace is not None else None,
+                priority=_dev_ptr(prio),
             )
             stream = torch.cuda.current_stream(dev).cuda_stream
             _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args), ctypes.c_void_p(stream)))
+            if sched is not None and ctr is not None:
+                sched.learn(cells, ctr[:, 1], ef_t, stopped)
         return ids, dists, ctr

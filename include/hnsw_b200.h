@@ -118,6 +118,11 @@ typedef struct hnsw_b200_search_args {
      * (0 and any: a constant threshold). */
     float stop_slope;
     int32_t stop_slope_from;
+    /* Start order: (nq,) int32 device array, or NULL for row order. Queries start in descending
+     * priority, equal priorities in row order (a stable sort on the low 16 bits, so values belong
+     * in [0, 65535]). Results do not depend on the order -- each query's search is independent --
+     * but the batch ends sooner when its longest queries start first. */
+    const int32_t *priority;
 } hnsw_b200_search_args_t;
 
 #define HNSW_B200_STOP_EVERY 16

@@ -191,6 +191,36 @@ def _workload(name: str):
     return arrays, int(meta["entry_point"]), int(meta["max_level"]), meta["params"]["metric"]
 
 
+def test_start_order_changes_no_result() -> None:
+    """Large batches on a cell-ordered graph start longest-predicted first (a priority array the
+    library sorts into the first work list): ids, distances and counters equal row order's, before
+    and after the per-cell costs are learned, and under arbitrary priorities."""
+    import torch
+
+    from hnsw_engine_b200 import graphs
+    from hnsw_engine_b200.schedule import MIN_QUERIES
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload("mix100k")
+    g = _index(arrays, ep, ml, metric, 16).device_graph
+    assert g._schedule is not None
+    q = torch.from_numpy(prepare(graphs.workload_queries("mix100k", nq=MIN_QUERIES + 904), metric)).cuda()
+    g.schedule = False
+    want = [t.cpu() for t in g.search(q, 10, 64)]
+    g.schedule = True
+    sched = g._schedule
+    for _ in range(3):  # the first batch starts in row order, the next ones by the learned costs
+        for a, b in zip(want, [t.cpu() for t in g.search(q, 10, 64)], strict=True):
+            assert torch.equal(a, b)
+    assert float(sched.count.sum()) == 3 * q.shape[0]
+    ef = torch.full((q.shape[0],), 64, dtype=torch.int32, device=q.device)
+    assert torch.unique(sched.priority(sched.cells(q), ef)).numel() > 1
+    sched.total.copy_(torch.rand_like(sched.total) * 2e6)  # arbitrary, partly clamped priorities
+    sched.count.fill_(1.0)
+    for a, b in zip(want, [t.cpu() for t in g.search(q, 10, 64)], strict=True):
+        assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("name", ["mix100k", "t100k"])
 def test_large_graph_per_query_ef_matches_oracle(name: str) -> None:
     from hnsw_engine_b200 import graphs, synthetic
