@@ -75,6 +75,9 @@ class SearchArgs(ctypes.Structure):
         ("stop_slope", ctypes.c_float),
         ("stop_slope_from", ctypes.c_int32),
         ("priority", ctypes.c_void_p),
+        ("cells", ctypes.c_void_p),
+        ("cell_cost", ctypes.c_void_p),
+        ("n_cells", ctypes.c_int32),
     ]
 
 
@@ -145,6 +148,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "hnsw_b200_upload_queries": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                                 ctypes.c_int32, ctypes.POINTER(ValueStats),
                                                 ctypes.c_void_p]),
+    "hnsw_b200_start_priority": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                                ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_version": (ctypes.c_char_p, []),
 }
 

@@ -1,0 +1,134 @@
+// Start order of a search batch: each query's cell -- its nearest pivot row -- and its predicted
+// length, the start priority that hnsw_b200_search sorts into its first work list. The search
+// kernel itself adds every finished query's expansions to the per-cell table (args->cells), so
+// the prediction needs this one launch per batch and no host round trip.
+//
+// Nearest pivot: squared L2 in float32 (a prediction input, so the rounding is of no
+// consequence), ties to the lower pivot index. A block takes 32 queries; each thread holds one
+// pivot of the current group of 256 and accumulates its distance to all 32 queries, whose values
+// arrive 32 dimensions at a time through shared memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+#include <string>
+
+#include "hnsw_b200.h"
+
+namespace hb {
+int fail(int code, const std::string &msg);
+}
+
+namespace hbs {
+
+constexpr int QT = 32;       // queries per block
+constexpr int THREADS = 256; // pivots per group (one per thread)
+constexpr int DC = 32;       // dimensions per staged chunk
+
+__global__ void __launch_bounds__(THREADS) start_priority_kernel(
+    const float *__restrict__ queries, int32_t nq, int32_t dim, const float *__restrict__ pivots,
+    int32_t n_cells, const double *__restrict__ cost, const int32_t *__restrict__ ef, float scale,
+    int32_t *__restrict__ cells, int32_t *__restrict__ priority) {
+    __shared__ float qs[QT][DC + 1];
+    __shared__ float wd[THREADS / 32][QT];
+    __shared__ int wi[THREADS / 32][QT];
+    __shared__ float best_d[QT];
+    __shared__ int best_i[QT];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int q0 = blockIdx.x * QT;
+    if (t < QT) {
+        best_d[t] = FLT_MAX;
+        best_i[t] = 0;
+    }
+    for (int g0 = 0; g0 < n_cells; g0 += THREADS) {
+        const int p = g0 + t;
+        const bool live = p < n_cells;
+        const float *prow = pivots + int64_t(live ? p : 0) * dim;
+        float acc[QT];
+#pragma unroll
+        for (int i = 0; i < QT; i++) acc[i] = 0.f;
+        for (int d0 = 0; d0 < dim; d0 += DC) {
+            __syncthreads();
+            for (int e = t; e < QT * DC; e += THREADS) {  // stage 32 queries x 32 dimensions
+                const int i = e / DC, d = e % DC;
+                const int qi = q0 + i, dd = d0 + d;
+                qs[i][d] = (qi < nq && dd < dim) ? queries[int64_t(qi) * dim + dd] : 0.f;
+            }
+            __syncthreads();
+            const int nd = min(DC, dim - d0);
+            for (int d = 0; d < nd; d++) {
+                const float pv = live ? __ldg(prow + d0 + d) : 0.f;
+#pragma unroll
+                for (int i = 0; i < QT; i++) {
+                    const float diff = qs[i][d] - pv;
+                    acc[i] = fmaf(diff, diff, acc[i]);
+                }
+            }
+        }
+        // argmin over this group's pivots, per query: within the warp, then across warps
+#pragma unroll
+        for (int i = 0; i < QT; i++) {
+            float v = live ? acc[i] : FLT_MAX;
+            int id = live ? p : INT32_MAX;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float v2 = __shfl_xor_sync(0xffffffffu, v, o);
+                const int id2 = __shfl_xor_sync(0xffffffffu, id, o);
+                if (v2 < v || (v2 == v && id2 < id)) {
+                    v = v2;
+                    id = id2;
+                }
+            }
+            if (lane == 0) {
+                wd[warp][i] = v;
+                wi[warp][i] = id;
+            }
+        }
+        __syncthreads();
+        if (t < QT) {
+            float v = best_d[t];
+            int id = best_i[t];
+            for (int w = 0; w < THREADS / 32; w++) {
+                if (wd[w][t] < v || (wd[w][t] == v && wi[w][t] < id)) {
+                    v = wd[w][t];
+                    id = wi[w][t];
+                }
+            }
+            best_d[t] = v;
+            best_i[t] = id;
+        }
+    }
+    __syncthreads();
+    if (t < QT && q0 + t < nq) {
+        const int q = q0 + t, c = best_i[t];
+        // expansions per unit of ef: plain searches' mean where they reached the cell, else the
+        // stopped searches' (0 for a cell nobody reached yet)
+        const double plain_n = cost[2 * int64_t(n_cells) + c];
+        const double ratio = plain_n > 0.0
+                                 ? cost[c] / plain_n
+                                 : cost[int64_t(n_cells) + c] / fmax(1.0, cost[3 * int64_t(n_cells) + c]);
+        const double key = fmin(65535.0, ratio * double(ef[q]) * double(scale));
+        cells[q] = c;
+        priority[q] = int32_t(key);
+    }
+}
+
+}  // namespace hbs
+
+extern "C" int hnsw_b200_start_priority(const float *queries, int64_t nq, int32_t dim,
+                                        const float *pivots, int32_t n_cells, const double *cost,
+                                        const int32_t *ef, float scale, int32_t *cells,
+                                        int32_t *priority, void *stream) {
+    if (nq < 0 || nq > INT32_MAX || dim < 1 || n_cells < 1 || !(scale >= 0.f))
+        return hb::fail(HNSW_B200_EINVAL, "start_priority: bad sizes");
+    if (nq == 0) return HNSW_B200_OK;
+    if (!queries || !pivots || !cost || !ef || !cells || !priority)
+        return hb::fail(HNSW_B200_EINVAL, "start_priority: null pointer");
+    const int blocks = int((nq + hbs::QT - 1) / hbs::QT);
+    hbs::start_priority_kernel<<<blocks, hbs::THREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+        queries, int32_t(nq), dim, pivots, n_cells, cost, ef, scale, cells, priority);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return hb::fail(HNSW_B200_ECUDA, std::string("start_priority: ") + cudaGetErrorString(e));
+    return HNSW_B200_OK;
+}

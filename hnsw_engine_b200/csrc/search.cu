@@ -130,6 +130,9 @@ struct SearchParams {
     int32_t queries_f64;
     const int32_t *qlist;  // work item -> query row (NULL: identity)
     int32_t n_work;
+    const int32_t *cells;  // per-cell cost learning (NULL: off)
+    double *cell_cost;     // (4, n_cells): plain sums, stopped sums, plain counts, stopped counts
+    int32_t n_cells;
     int32_t k, k_search;
     const int32_t *ef;
     int32_t ef_cap;
@@ -1550,6 +1553,15 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
                 P.out_ctr[2 * int64_t(q)] = C.ndist;
                 P.out_ctr[2 * int64_t(q) + 1] = C.nhops;
             }
+            if (P.cells) {  // the start order's per-cell cost table; cells outside it are skipped
+                const int c = P.cells[q];
+                if (c >= 0 && c < P.n_cells) {
+                    const int64_t tb = P.stop_mlp ? 1 : 0;
+                    atomicAdd(P.cell_cost + tb * P.n_cells + c,
+                              double(C.nhops) / double(max(1, __ldg(P.ef + q))));
+                    atomicAdd(P.cell_cost + (2 + tb) * P.n_cells + c, 1.0);
+                }
+            }
         }
         __syncwarp();
     }
@@ -1868,6 +1880,9 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.trace_count = a->trace_count;
     P.trace_hops = a->trace_hops;
     P.trace_cap = a->trace_cap;
+    P.cells = a->cell_cost && a->n_cells > 0 ? a->cells : nullptr;
+    P.cell_cost = a->cell_cost;
+    P.n_cells = a->n_cells;
     P.trace_k = 16;
     // One lane per neighbour's row: a win unless the filter is very selective, where most rows it
     // would fetch early belong to neighbours already visited.
@@ -2141,6 +2156,9 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     P.trace_count = a->trace_count;
     P.trace_hops = a->trace_hops;
     P.trace_cap = a->trace_cap;
+    P.cells = a->cell_cost && a->n_cells > 0 ? a->cells : nullptr;
+    P.cell_cost = a->cell_cost;
+    P.n_cells = a->n_cells;
     P.trace_k = 16;
     P.lane_rows = 1;
     int rc = 0;

@@ -490,10 +490,8 @@ class DeviceGraph:
                                        and nq >= MIN_QUERIES and bitmap is None and not use_codes
                                        and trace is None) else None
             cells = prio = None
-            stopped = stop is not None
             if sched is not None:
-                cells = sched.cells(q)
-                prio = sched.priority(cells, ef_t, stopped)
+                cells, prio = sched.start(q, ef_t)
             if out is None:
                 ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
                 dists = torch.empty((nq, k), dtype=torch.float64, device=dev)
@@ -526,9 +524,10 @@ class DeviceGraph:
                 trace_count=_dev_ptr(trace[2]) if trace is not None else None,
                 trace_hops=_dev_ptr(trace[3]) if trace is not None else None,
                 priority=_dev_ptr(prio),
+                cells=_dev_ptr(cells),
+                cell_cost=_dev_ptr(sched.cost) if sched is not None else None,
+                n_cells=sched.n_cells if sched is not None else 0,
             )
             stream = torch.cuda.current_stream(dev).cuda_stream
             _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args), ctypes.c_void_p(stream)))
-            if sched is not None and ctr is not None:
-                sched.learn(cells, ctr[:, 1], ef_t, stopped)
         return ids, dists, ctr

@@ -123,6 +123,13 @@ typedef struct hnsw_b200_search_args {
      * in [0, 65535]). Results do not depend on the order -- each query's search is independent --
      * but the batch ends sooner when its longest queries start first. */
     const int32_t *priority;
+    /* Per-cell cost learning: with cells ((nq,) device, each query's cell in [0, n_cells), as
+     * hnsw_b200_start_priority gives it) every finished query adds its expansions per unit of
+     * efSearch, and 1, to cell_cost ((4, n_cells) float64 device: plain sums, stopped sums,
+     * plain counts, stopped counts; "stopped" = searched with stop_mlp). NULL: no learning. */
+    const int32_t *cells;
+    double *cell_cost;
+    int32_t n_cells;
 } hnsw_b200_search_args_t;
 
 #define HNSW_B200_STOP_EVERY 16
@@ -262,6 +269,15 @@ typedef struct {
 } hnsw_b200_value_stats_t;
 int hnsw_b200_upload_queries(const float *src, float *dst, int64_t count, int32_t threads,
                              hnsw_b200_value_stats_t *out, void *stream);
+
+/* Start priorities for hnsw_b200_search (one launch): each query's cell -- its nearest of the
+ * n_cells float32 pivot rows (squared L2 in float32, ties to the lower index) -- into cells, and
+ * min(65535, ratio * ef[q] * scale) into priority, where ratio is the cell's expansions per unit
+ * of efSearch from cell_cost (the table hnsw_b200_search learns: the plain searches' mean where
+ * plain counts are nonzero, else the stopped searches'). queries: (nq, dim) float32 device. */
+int hnsw_b200_start_priority(const float *queries, int64_t nq, int32_t dim, const float *pivots,
+                             int32_t n_cells, const double *cell_cost, const int32_t *ef,
+                             float scale, int32_t *cells, int32_t *priority, void *stream);
 
 /* Library version string. */
 const char *hnsw_b200_version(void);

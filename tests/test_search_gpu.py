@@ -212,11 +212,11 @@ def test_start_order_changes_no_result() -> None:
     for _ in range(3):  # the first batch starts in row order, the next ones by the learned costs
         for a, b in zip(want, [t.cpu() for t in g.search(q, 10, 64)], strict=True):
             assert torch.equal(a, b)
-    assert float(sched.count.sum()) == 3 * q.shape[0]
+    assert float(sched.cost[2].sum()) == 3 * q.shape[0]  # plain query counts
     ef = torch.full((q.shape[0],), 64, dtype=torch.int32, device=q.device)
-    assert torch.unique(sched.priority(sched.cells(q), ef)).numel() > 1
-    sched.total.copy_(torch.rand_like(sched.total) * 2e6)  # arbitrary, partly clamped priorities
-    sched.count.fill_(1.0)
+    assert torch.unique(sched.start(q, ef)[1]).numel() > 1
+    sched.cost[0].copy_(torch.rand_like(sched.cost[0]) * 300)  # arbitrary, partly clamped priorities
+    sched.cost[2].fill_(1.0)
     for a, b in zip(want, [t.cpu() for t in g.search(q, 10, 64)], strict=True):
         assert torch.equal(a, b)
 
