@@ -7,9 +7,11 @@
 // float32 -- exact for byte-valued data at d = 128, and a prediction input in any case, so the
 // rounding is of no consequence; ties go to the lower pivot index. A block of 128 threads takes
 // 16 queries; each thread holds two pivots of the current group of 256 and accumulates their dot
-// products with all 16 queries, whose values arrive 32 dimensions at a time through shared memory
-// (transposed, read as float4 broadcasts). 10,000 queries make 625 blocks: one wave at 5 blocks
-// per SM.
+// products with all 16 queries. Queries and pivots arrive 32 dimensions at a time through shared
+// memory: rows read whole (coalesced) and stored transposed, the queries read back as float4
+// broadcasts, the pivots one word per thread (the pivot tile's rows are padded by one word, so
+// the transposing stores and the reads are free of bank conflicts). 10,000 queries make 625
+// blocks: one wave.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,6 +37,7 @@ __global__ void __launch_bounds__(THREADS) start_priority_kernel(
     int32_t n_cells, const double *__restrict__ cost, const int32_t *__restrict__ ef, float scale,
     int32_t *__restrict__ cells, int32_t *__restrict__ priority) {
     __shared__ __align__(16) float qs[DC][QT];  // [dimension][query]
+    __shared__ float ps[DC][GROUP + 1];         // [dimension][pivot of the group]
     __shared__ float wd[THREADS / 32][QT];
     __shared__ int wi[THREADS / 32][QT];
     __shared__ float best_d[QT];
@@ -48,8 +51,6 @@ __global__ void __launch_bounds__(THREADS) start_priority_kernel(
     for (int g0 = 0; g0 < n_cells; g0 += GROUP) {
         const int pa = g0 + t, pb = g0 + THREADS + t;
         const bool la = pa < n_cells, lb = pb < n_cells;
-        const float *ra = pivots + int64_t(la ? pa : 0) * dim;
-        const float *rb = pivots + int64_t(lb ? pb : 0) * dim;
         float acc_a[QT], acc_b[QT];
 #pragma unroll
         for (int i = 0; i < QT; i++) {
@@ -64,11 +65,16 @@ __global__ void __launch_bounds__(THREADS) start_priority_kernel(
                 const int qi = q0 + i, dd = d0 + d;
                 qs[d][i] = (qi < nq && dd < dim) ? queries[int64_t(qi) * dim + dd] : 0.f;
             }
+            for (int e = t; e < GROUP * DC; e += THREADS) {  // and 256 pivots x 32 dimensions
+                const int j = e / DC, d = e % DC;
+                const int pj = g0 + j, dd = d0 + d;
+                ps[d][j] = (pj < n_cells && dd < dim) ? __ldg(pivots + int64_t(pj) * dim + dd) : 0.f;
+            }
             __syncthreads();
             const int nd = min(DC, dim - d0);
             for (int d = 0; d < nd; d++) {
-                const float va = la ? __ldg(ra + d0 + d) : 0.f;
-                const float vb = lb ? __ldg(rb + d0 + d) : 0.f;
+                const float va = ps[d][t];
+                const float vb = ps[d][THREADS + t];
                 na = fmaf(va, va, na);
                 nb = fmaf(vb, vb, nb);
                 const float4 *qv = reinterpret_cast<const float4 *>(qs[d]);
