@@ -266,7 +266,7 @@ def main() -> None:
         pg = dist
 
     from hnsw_engine_b200 import HNSWIndex, graphs, synthetic
-    from hnsw_engine_b200.learned_stop import tune_threshold
+    from hnsw_engine_b200.learned_stop import audited_search, stopped_search, tune_threshold
     from hnsw_engine_b200.train_stop import load_or_train
     from hnsw_engine_b200.validation import prepare
 
@@ -382,6 +382,20 @@ def main() -> None:
     e2e_value = job_throughput(world, nq, 1, e2e_ms)
     assert np.array_equal(e_ids, ids_o.cpu().numpy()), "e2e results differ from device results"
 
+    # Held out: the threshold tuned on the validation queries (not these), its recall here, and
+    # how often the per-batch audit (2% of each batch against the exact k-NN) falls back to plain
+    # fixed ef, over ten batches of a tenth of the queries.
+    ho_ids, ho_d, ho_c = stopped_search(g, q_dev, k, cap, packed, val_threshold, net.slope,
+                                        net.slope_from)
+    ho_rec = recall_of(ho_ids.cpu().numpy(), ho_d.cpu().numpy(), gt_ids, gt_d, k)
+    net.threshold = val_threshold
+    audits = []
+    for part_i, part in enumerate(np.array_split(np.arange(nq), 10)):
+        _, _, fell, arec = audited_search(g, q_dev[torch.from_numpy(part).to(dev)], k, cap, net,
+                                          ef_op, RECALL_TARGET, seed=part_i)
+        audits.append((bool(fell), float(arec)))
+    net.threshold = thr
+
     # Per-query efSearch uniform on 32..512 (the batched-at-scale configuration).
     pq = synthetic.per_query_ef(nq, seed=11, low=32, high=512)
     pq_dev = torch.from_numpy(pq).to(dev)
@@ -423,7 +437,15 @@ def main() -> None:
                 "learned_stop": {"ef_cap": cap, "threshold": thr, "recall_at_10": rec_l,
                                  "threshold_slope": net.slope, "slope_from_hops": net.slope_from,
                                  "qps": value, "mean_hops": hops_l,
-                                 "validation_threshold": val_threshold},
+                                 "validation_threshold": val_threshold,
+                                 "held_out": {
+                                     "threshold": val_threshold,
+                                     "recall_at_10": ho_rec,
+                                     "mean_hops": float(ho_c[:, 1].float().mean()),
+                                     "audit_batches": len(audits),
+                                     "audit_fallbacks": sum(f for f, _ in audits),
+                                     "audit_sample_recalls": [r for _, r in audits],
+                                 }},
                 "plain_fixed_ef": {"ef": ef_op, "recall_at_10": rec_p, "qps": plain_qps,
                                    "mean_hops": hops_p,
                                    "achieved_gbs": alg_bytes_plain / (total_p / args.steps / 1000.0) / 1e9},

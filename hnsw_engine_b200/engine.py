@@ -124,6 +124,7 @@ class DeviceGraph:
         # False to start queries in row order. Results are the same either way.
         self.schedule = True
         self._schedule: CellSchedule | None = None
+        self._priority_launches = 0
         self._internal: dict[str, Any] = {}
         if validate_M is not None:  # before anything follows the links
             self._validate_on_device(arrays["levels"], int(validate_M))
@@ -280,7 +281,9 @@ class DeviceGraph:
 
     @property
     def last_launches(self) -> int:
-        return int(self.lib.hnsw_b200_last_launches(self._handle))
+        """This library's kernel launches in the last search: the start-priority kernel, when it
+        ran, and those of hnsw_b200_search."""
+        return int(self.lib.hnsw_b200_last_launches(self._handle)) + self._priority_launches
 
     # ------------------------------------------------------------------ arithmetic selection
     def choose_mode(self, queries: NDArray[Any], codes: bool) -> int:
@@ -490,8 +493,10 @@ class DeviceGraph:
                                        and nq >= MIN_QUERIES and bitmap is None and not use_codes
                                        and trace is None) else None
             cells = prio = None
+            self._priority_launches = 0
             if sched is not None:
                 cells, prio = sched.start(q, ef_t)
+                self._priority_launches = 1
             if out is None:
                 ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
                 dists = torch.empty((nq, k), dtype=torch.float64, device=dev)
