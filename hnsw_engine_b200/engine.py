@@ -489,14 +489,20 @@ class DeviceGraph:
             rq = None
             if rerank_queries is not None:
                 rq = to_device(rerank_queries, torch.float32, dev)
+            # Start order: cells from the float32 queries (code-space searches: their rerank
+            # queries). Filtered searches read the order but do not learn: a filter scales every
+            # query's cost by about the same factor, so the unfiltered cell ranking still holds,
+            # but their expansions would distort the table.
+            cell_q = q if not use_codes else rq
             sched = self._schedule if (self.schedule and self._schedule is not None
-                                       and nq >= MIN_QUERIES and bitmap is None and not use_codes
-                                       and trace is None) else None
+                                       and nq >= MIN_QUERIES and trace is None
+                                       and cell_q is not None) else None
             cells = prio = None
             self._priority_launches = 0
             if sched is not None:
-                cells, prio = sched.start(q, ef_t)
+                cells, prio = sched.start(cell_q, ef_t)
                 self._priority_launches = 1
+            learn = sched is not None and bitmap is None
             if out is None:
                 ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
                 dists = torch.empty((nq, k), dtype=torch.float64, device=dev)
@@ -529,9 +535,9 @@ class DeviceGraph:
                 trace_count=_dev_ptr(trace[2]) if trace is not None else None,
                 trace_hops=_dev_ptr(trace[3]) if trace is not None else None,
                 priority=_dev_ptr(prio),
-                cells=_dev_ptr(cells),
-                cell_cost=_dev_ptr(sched.cost) if sched is not None else None,
-                n_cells=sched.n_cells if sched is not None else 0,
+                cells=_dev_ptr(cells) if learn else None,
+                cell_cost=_dev_ptr(sched.cost) if learn else None,
+                n_cells=sched.n_cells if learn else 0,
             )
             stream = torch.cuda.current_stream(dev).cuda_stream
             _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args), ctypes.c_void_p(stream)))

@@ -219,6 +219,24 @@ def test_start_order_changes_no_result() -> None:
     sched.cost[2].fill_(1.0)
     for a, b in zip(want, [t.cpu() for t in g.search(q, 10, 64)], strict=True):
         assert torch.equal(a, b)
+    # filtered batches follow the order without learning from it; code-space batches (with a
+    # fused rerank) take their cells from the float32 rerank queries
+    mask = np.random.default_rng(4).random(arrays["vectors"].shape[0]) < 0.3
+    g.attach_codes(np.asarray(arrays["vectors"], dtype=np.uint8))  # integer 0..255: lossless
+    runs = {"filtered": dict(allowed=mask),
+            "codes": dict(use_codes=True, k_search=64, rerank_queries=q)}
+    for name, kw in runs.items():
+        qq = q.double() if name == "codes" else q
+        g.schedule = False
+        row_order = [t.cpu() for t in g.search(qq, 10, 64, **kw)]
+        g.schedule = True
+        before = sched.cost.clone()
+        started = [t.cpu() for t in g.search(qq, 10, 64, **kw)]
+        assert g.last_launches >= 2, name  # the priority kernel ran
+        for a, b in zip(row_order, started, strict=True):
+            assert torch.equal(a, b), name
+        if name == "filtered":
+            assert torch.equal(sched.cost, before)
 
 
 @pytest.mark.parametrize("name", ["mix100k", "t100k"])
