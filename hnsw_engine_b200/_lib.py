@@ -147,7 +147,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                                                 ctypes.c_void_p]),
     "hnsw_b200_upload_queries": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                                 ctypes.c_int32, ctypes.POINTER(ValueStats),
-                                                ctypes.c_void_p]),
+                                                ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_start_priority": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                                                 ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p,

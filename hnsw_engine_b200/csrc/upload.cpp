@@ -7,9 +7,11 @@
 // _validation.py:30-35, "contains NaN or infinite values") and the float32 cast of
 // metrics.py:49-53, a copy for float32 rows.
 //
-// Why not stage into page-locked memory on the pool threads and DMA from there: measured on the
-// B200 hosts (16 vCPUs), a DMA read of 5 MB of page-locked memory just written by 8 threads took
-// 0.90 ms against 0.12 ms after a single-thread write; the plain pageable copy takes 0.30 ms.
+// With a page-locked staging buffer the pool threads also copy the rows into it, with streaming
+// (non-temporal) stores, and one asynchronous DMA follows. Measured on the B200 hosts (16 vCPUs),
+// 5 MB: the pageable copy takes 0.30 ms; staging by 4 threads plus the DMA 0.22 ms with streaming
+// stores, but 0.86 ms with ordinary ones -- a DMA read of lines still dirty in other cores' caches
+// is slow there.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -109,15 +111,18 @@ struct Part {
 //  - integer: x clamped to [-2^23, 2^23] survives truncation to int32 and back (every float32 of
 //    larger magnitude is an integer; the clamp sends NaN to -2^23, an integer);
 //  - min / max: MINPS / MAXPS with the running value second, so a NaN input leaves it unchanged.
-Part scan(const float *__restrict src, int64_t b, int64_t e) {
+Part scan(const float *__restrict src, float *__restrict stage, int64_t b, int64_t e) {
     const __m128 absmask = _mm_castsi128_ps(_mm_set1_epi32(0x7fffffff));
     const __m128 big = _mm_set1_ps(FLT_MAX);
     const __m128 c_hi = _mm_set1_ps(8388608.0f), c_lo = _mm_set1_ps(-8388608.0f);
     __m128 lo = _mm_set1_ps(FLT_MAX), hi = _mm_set1_ps(-FLT_MAX);
     __m128i bad = _mm_setzero_si128(), frac = _mm_setzero_si128();
     int64_t i = b;
+    // stage + b is 16-byte aligned (parts start at multiples of 16 values; the buffer is
+    // page-locked memory, page aligned)
     for (; i + 4 <= e; i += 4) {
         const __m128 x = _mm_loadu_ps(src + i);
+        if (stage) _mm_stream_ps(stage + i, x);
         bad = _mm_or_si128(bad, _mm_castps_si128(_mm_cmpnle_ps(_mm_and_ps(x, absmask), big)));
         const __m128 y = _mm_min_ps(_mm_max_ps(x, c_lo), c_hi);
         const __m128 t = _mm_cvtepi32_ps(_mm_cvttps_epi32(y));
@@ -137,6 +142,7 @@ Part scan(const float *__restrict src, int64_t b, int64_t e) {
     }
     for (; i < e; ++i) {  // the last values, one at a time by the same rules
         const float x = src[i];
+        if (stage) stage[i] = x;
         if (!(std::fabs(x) <= FLT_MAX)) {
             p.finite = false;
             continue;
@@ -146,6 +152,7 @@ Part scan(const float *__restrict src, int64_t b, int64_t e) {
         p.lo = std::min(p.lo, x);
         p.hi = std::max(p.hi, x);
     }
+    if (stage) _mm_sfence();  // the streaming stores are visible before the DMA is issued
     return p;
 }
 
@@ -153,33 +160,40 @@ Part scan(const float *__restrict src, int64_t b, int64_t e) {
 
 extern "C" int hnsw_b200_upload_queries(const float *src, float *dst, int64_t count,
                                         int32_t threads, hnsw_b200_value_stats_t *out,
-                                        void *stream) {
+                                        float *staging, void *stream) {
     if (count < 0 || out == nullptr || (count > 0 && src == nullptr))
         return hb::fail(HNSW_B200_EINVAL, "upload_queries: bad argument");
+    if (staging != nullptr && (reinterpret_cast<uintptr_t>(staging) & 15u) != 0)
+        return hb::fail(HNSW_B200_EINVAL, "upload_queries: staging must be 16-byte aligned");
+    float *stage = dst != nullptr ? staging : nullptr;
     cudaError_t copy_err = cudaSuccess;
-    const std::function<void()> copy = [&] {
-        if (dst != nullptr && count > 0)
+    const std::function<void()> copy = [&] {  // pageable copy, concurrent with the scan
+        if (dst != nullptr && stage == nullptr && count > 0)
             copy_err = cudaMemcpyAsync(dst, src, size_t(count) * sizeof(float),
                                        cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream));
     };
+    const std::function<void()> nothing = [] {};
     // at least 64K values (256 KB) per part: below that a wake-up costs more than the scan
     constexpr int64_t MIN_PART = 65536;
     int parts = int(std::min<int64_t>(std::max(1, threads), (count + MIN_PART - 1) / MIN_PART));
     std::vector<Part> res;
     if (parts <= 1) {
         copy();
-        res.push_back(scan(src, 0, count));
+        res.push_back(scan(src, stage, 0, count));
     } else {
         HostPool &p = pool();
         parts = std::min(parts, p.workers());
         res.resize(size_t(parts));
-        const int64_t per = (count + parts - 1) / parts;
+        const int64_t per = ((count + parts - 1) / parts + 15) / 16 * 16;  // aligned part starts
         const std::function<void(int)> job = [&](int i) {
             const int64_t b = std::min(count, int64_t(i) * per);
-            res[size_t(i)] = scan(src, b, std::min(count, b + per));
+            res[size_t(i)] = scan(src, stage, b, std::min(count, b + per));
         };
-        p.run(parts, job, copy);
+        p.run(parts, job, stage ? nothing : copy);
     }
+    if (stage != nullptr && count > 0)  // one asynchronous DMA of the staged rows
+        copy_err = cudaMemcpyAsync(dst, stage, size_t(count) * sizeof(float),
+                                   cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream));
     if (copy_err != cudaSuccess)
         return hb::fail(HNSW_B200_ECUDA, std::string("upload_queries: ") + cudaGetErrorString(copy_err));
     Part all;

@@ -125,6 +125,9 @@ class DeviceGraph:
         self.schedule = True
         self._schedule: CellSchedule | None = None
         self._priority_launches = 0
+        # page-locked staging of uploaded query batches, and the end of the last DMA from it
+        self._stage: torch.Tensor | None = None
+        self._stage_done = torch.cuda.Event()
         self._internal: dict[str, Any] = {}
         if validate_M is not None:  # before anything follows the links
             self._validate_on_device(arrays["levels"], int(validate_M))
@@ -318,22 +321,36 @@ class DeviceGraph:
         return bool(bound < EXACT_LIMIT)
 
     def upload_queries(self, src: NDArray[np.float32], dst: torch.Tensor | None,
-                       threads: int = UPLOAD_THREADS) -> _lib.ValueStats:
+                       threads: int = UPLOAD_THREADS, staged: bool = True) -> _lib.ValueStats:
         """Copy C-contiguous float32 host queries into the device tensor ``dst`` on the current
         stream (``None``: no copy) and return their statistics (finite, integer, min, max), read
-        on host threads in the library while the copy runs."""
+        on host threads in the library.
+
+        ``staged``: the threads also copy the rows into this graph's page-locked staging buffer
+        and one asynchronous DMA follows (faster than the pageable copy); the buffer is reused
+        only once the previous DMA from it has completed."""
         st = _lib.ValueStats()
         if dst is None:
             _lib.check(self.lib.hnsw_b200_upload_queries(src.ctypes.data, None, src.size,
-                                                          int(threads), ctypes.byref(st), None))
+                                                          int(threads), ctypes.byref(st), None, None))
             return st
         if dst.numel() != src.size or dst.dtype != torch.float32 or not dst.is_contiguous():
             raise ValueError("dst must be a contiguous float32 device tensor of src's size")
         with torch.cuda.device(self.device):
-            stream = torch.cuda.current_stream(self.device).cuda_stream
+            stream = torch.cuda.current_stream(self.device)
+            stage = None
+            if staged:
+                if self._stage is None or self._stage.numel() < src.size:
+                    self._stage = torch.empty(max(src.size, 1 << 20), dtype=torch.float32,
+                                              pin_memory=True)
+                else:
+                    self._stage_done.synchronize()  # the previous DMA from it has finished
+                stage = self._stage
             _lib.check(self.lib.hnsw_b200_upload_queries(
                 src.ctypes.data, _dev_ptr(dst), src.size, int(threads), ctypes.byref(st),
-                ctypes.c_void_p(stream)))
+                _dev_ptr(stage), ctypes.c_void_p(stream.cuda_stream)))
+            if stage is not None:
+                self._stage_done.record(stream)
         return st
 
     def mode_from_stats(self, st: _lib.ValueStats, queries: NDArray[np.float32]) -> int:

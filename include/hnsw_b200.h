@@ -254,21 +254,25 @@ int hnsw_b200_quant_encode(const float *vectors, int64_t n, int32_t dim, const d
 int hnsw_b200_validate_graph(const hnsw_b200_graph_t *graph, const int64_t *levels, int32_t M,
                              void *scratch, uint32_t *flags_out, void *stream);
 
-/* Upload of a float32 query batch: copies `count` values from host src (pageable) to device dst
- * with cudaMemcpyAsync on `stream` (NULL dst: no copy, no GPU work), and meanwhile reports in *out
- * whether every value is finite and an integer, with their minimum and maximum, from a read of src
- * on up to `threads` host threads. Replaces, for contiguous float32 batches, the host validator's
- * NaN/inf pass (_validation.py:30-35) and the float32 cast of metrics.py:49-53 (a copy for float32
- * rows); the statistics select the distance arithmetic without reading the queries back from the
- * GPU. min and max are meaningful only when finite is 1. src may be reused on return (the copy is
- * staged by then); dst is complete in stream order. */
+/* Upload of a float32 query batch to device dst on `stream` (NULL dst: no copy, no GPU work), and
+ * in *out whether every value is finite and an integer, with their minimum and maximum, from a
+ * read of src on up to `threads` host threads. Replaces, for contiguous float32 batches, the host
+ * validator's NaN/inf pass (_validation.py:30-35) and the float32 cast of metrics.py:49-53 (a copy
+ * for float32 rows); the statistics select the distance arithmetic without reading the queries
+ * back from the GPU. min and max are meaningful only when finite is 1.
+ *   - staging NULL: a pageable cudaMemcpyAsync from src, concurrent with the read;
+ *   - staging: page-locked host memory of `count` floats, 16-byte aligned, not in use by an
+ *     earlier copy; the threads copy src into it as they read (streaming stores) and one
+ *     asynchronous DMA follows. The caller keeps it untouched until the copy completes in stream
+ *     order.
+ * src may be reused on return; dst is complete in stream order. */
 typedef struct {
     int32_t finite;   /* 1 if no value is NaN or +-inf */
     int32_t integer;  /* 1 if every value is an integer */
     double min, max;  /* over all values (0 for count == 0) */
 } hnsw_b200_value_stats_t;
 int hnsw_b200_upload_queries(const float *src, float *dst, int64_t count, int32_t threads,
-                             hnsw_b200_value_stats_t *out, void *stream);
+                             hnsw_b200_value_stats_t *out, float *staging, void *stream);
 
 /* Start priorities for hnsw_b200_search (one launch): each query's cell -- its nearest of the
  * n_cells float32 pivot rows (squared L2 in float32, ties to the lower index) -- into cells, and

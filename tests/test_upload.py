@@ -23,7 +23,8 @@ def _scan(lib, x: np.ndarray, threads: int):
 
     x = np.ascontiguousarray(x, dtype=np.float32)
     st = ValueStats()
-    check(lib.hnsw_b200_upload_queries(x.ctypes.data, None, x.size, threads, ctypes.byref(st), None))
+    check(lib.hnsw_b200_upload_queries(x.ctypes.data, None, x.size, threads, ctypes.byref(st), None,
+                                       None))
     return st
 
 
@@ -68,6 +69,10 @@ def test_upload_rejects_null_arguments(lib) -> None:
     from hnsw_engine_b200._lib import ValueStats
 
     st = ValueStats()
-    assert lib.hnsw_b200_upload_queries(None, None, 4, 1, ctypes.byref(st), None) == -1
-    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, None, None) == -1
-    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, ctypes.byref(st), None) == 0
+    assert lib.hnsw_b200_upload_queries(None, None, 4, 1, ctypes.byref(st), None, None) == -1
+    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, None, None, None) == -1
+    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, ctypes.byref(st), None, None) == 0
+    # a misaligned staging buffer is refused before any copy
+    buf = (ctypes.c_float * 8)()
+    assert lib.hnsw_b200_upload_queries(None, None, 0, 1, ctypes.byref(st),
+                                        ctypes.addressof(buf) + 4, None) == -1
