@@ -133,6 +133,9 @@ class DeviceGraph:
             self._validate_on_device(arrays["levels"], int(validate_M))
         if self.locality:
             self._build_internal_order()
+        elif self.n >= LOCALITY_MIN_NODES:  # the start order alone: pivots, no memory reorder
+            with torch.cuda.device(self.device):
+                self._schedule = CellSchedule(self._pivot_rows())
         self._handle = ctypes.c_void_p()
         self._open()
 
@@ -166,10 +169,8 @@ class DeviceGraph:
 
         dev = self.device
         n = self.n
-        cells = min(LOCALITY_CELLS, n)
-        pick = np.sort(np.random.default_rng(0).choice(n, cells, replace=False))
         with torch.cuda.device(dev):
-            pivots = self.vectors[torch.from_numpy(pick).to(dev)].contiguous()
+            pivots = self._pivot_rows()
             nearest, _ = exact_search(pivots, self.vectors, 1, "l2")
             order = torch.sort(nearest[:, 0], stable=True).indices  # internal -> original
             new_of_old = torch.empty_like(order)
@@ -202,6 +203,13 @@ class DeviceGraph:
             self._schedule = CellSchedule(pivots)
         self.order = order
         self._order_host = order.cpu().numpy()
+
+    def _pivot_rows(self) -> torch.Tensor:
+        """The cells' pivots: LOCALITY_CELLS rows sampled without replacement (seed 0), in row
+        order, as float32 device rows."""
+        cells = min(LOCALITY_CELLS, self.n)
+        pick = np.sort(np.random.default_rng(0).choice(self.n, cells, replace=False))
+        return self.vectors[torch.from_numpy(pick).to(self.device)].contiguous()
 
     def internal_mask(self, mask: NDArray[np.bool_]) -> NDArray[np.bool_]:
         """A filter mask over original ids, rearranged into the internal node order."""
