@@ -239,6 +239,30 @@ def test_start_order_changes_no_result() -> None:
             assert torch.equal(sched.cost, before)
 
 
+def test_start_order_without_cell_order_changes_no_result() -> None:
+    """A large float graph (no cell order: the float64 kernel) gets pivots for the start order
+    alone; fixed and per-query ef give row order's ids, distances and counters."""
+    import torch
+
+    from hnsw_engine_b200 import graphs, synthetic
+    from hnsw_engine_b200.schedule import MIN_QUERIES
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload("t100k")
+    g = _index(arrays, ep, ml, metric, 16).device_graph
+    assert g._schedule is not None and not g.locality
+    q = torch.from_numpy(prepare(graphs.workload_queries("t100k", nq=MIN_QUERIES), metric)).cuda()
+    pq = torch.from_numpy(synthetic.per_query_ef(MIN_QUERIES, seed=3, low=16, high=128)).cuda()
+    for ef in (48, pq):
+        g.schedule = False
+        want = [t.cpu() for t in g.search(q, 10, ef)]
+        g.schedule = True
+        for _ in range(2):
+            for a, b in zip(want, [t.cpu() for t in g.search(q, 10, ef)], strict=True):
+                assert torch.equal(a, b)
+    assert float(g._schedule.cost[2].sum()) == 4 * MIN_QUERIES
+
+
 @pytest.mark.parametrize("name", ["mix100k", "t100k"])
 def test_large_graph_per_query_ef_matches_oracle(name: str) -> None:
     from hnsw_engine_b200 import graphs, synthetic
