@@ -500,6 +500,7 @@ __device__ __forceinline__ float funkey(uint32_t k) {
 __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32_t cap, int32_t nq,
                            int32_t k, const float *margin, float *out_thr, float *out_tau) {
     __shared__ uint32_t hist[256];
+    __shared__ uint32_t wsum[8];  // per-warp bin totals (blockDim.x == 256)
     __shared__ uint32_t s_prefix, s_rank;
     const int q = blockIdx.x;
     if (q >= nq) return;
@@ -522,15 +523,24 @@ __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32
             if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            int bin = 0;
-            for (; bin < 256; bin++) {
-                if (acc + hist[bin] >= rank) break;
-                acc += hist[bin];
-            }
-            s_prefix = prefix | (uint32_t(bin) << shift);
-            s_rank = rank - acc;
+        // The bucket holding the rank-th key: the bin whose counts before it are below rank and
+        // through it reach rank. A prefix sum over the 256 bins (one per thread: a warp scan,
+        // then the 8 warp totals), so exactly one thread finds it.
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint32_t c = hist[threadIdx.x];
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        for (int w = 0; w < warp; w++) incl += wsum[w];
+        const uint32_t excl = incl - c;
+        if (excl < rank && rank <= incl) {
+            s_prefix = prefix | (uint32_t(threadIdx.x) << shift);
+            s_rank = rank - excl;
         }
         __syncthreads();
         prefix = s_prefix;
