@@ -239,6 +239,31 @@ def test_start_order_changes_no_result() -> None:
             assert torch.equal(sched.cost, before)
 
 
+def test_overflow_retries_keep_results_in_start_order() -> None:
+    """A filtered batch told its filter allows every node (allowed_fraction = 1) gets scratch sized
+    for an unfiltered search: most queries overflow their candidate spill or visited set, are
+    flagged (never written past) and re-run with four times the scratch. The results equal those of
+    a batch sized for its real selectivity, with the start order on."""
+    import torch
+
+    from hnsw_engine_b200 import graphs
+    from hnsw_engine_b200.engine import pack_mask
+    from hnsw_engine_b200.schedule import MIN_QUERIES
+    from hnsw_engine_b200.validation import prepare
+
+    arrays, ep, ml, metric = _workload("mix100k")
+    g = _index(arrays, ep, ml, metric, 16).device_graph
+    q = torch.from_numpy(prepare(graphs.workload_queries("mix100k", nq=MIN_QUERIES), metric)).cuda()
+    mask = np.random.default_rng(6).random(arrays["vectors"].shape[0]) < 0.02
+    g.search(q, 10, 64)  # learn some cell costs, so the filtered batches start in an order
+    want = [t.cpu() for t in g.search(q, 10, 64, allowed=mask)]
+    bits = torch.from_numpy(pack_mask(g.internal_mask(mask)).view(np.int32)).cuda()
+    got = [t.cpu() for t in g.search(q, 10, 64, allowed=bits, allowed_fraction=1.0)]
+    assert g.last_launches > 3  # overflowed queries were collected and searched again
+    for a, b in zip(want, got, strict=True):
+        assert torch.equal(a, b)
+
+
 def test_start_order_without_cell_order_changes_no_result() -> None:
     """A large float graph (no cell order: the float64 kernel) gets pivots for the start order
     alone; fixed and per-query ef give row order's ids, distances and counters."""
