@@ -482,6 +482,10 @@ class DeviceGraph:
         buffers ``(features (nq, cap, 12) f32, first 16 result distances (nq, cap, 16) f64,
         count (nq,) i32, hops (nq,) i32)``
         filled with the stop features every 16 layer-0 expansions.
+
+        Batches of at least ``schedule.MIN_QUERIES`` on graphs of at least ``LOCALITY_MIN_NODES``
+        nodes start longest-predicted first (``self.schedule``; see :mod:`.schedule`); results
+        do not depend on it.
         """
         dev = self.device
         nq = int(queries.shape[0])
