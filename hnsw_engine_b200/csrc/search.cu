@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -206,9 +207,15 @@ __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filt
     return b;
 }
 
-struct Ctx {
+// D: the type of the result distances Rd. Unfiltered byte searches use float -- their distances
+// are integers of magnitude at most 128 * 255^2 < 2^24, exact in float32, so order and ties are
+// unchanged -- halving the result list's shuffles and shared-memory traffic and keeping its
+// compares off the FP64 pipe. Every other search uses double.
+template <typename D>
+struct CtxT {
+    using dist_t = D;
     int lane;
-    double *Rd;
+    D *Rd;
     int32_t *Ri;  // original id of each result (ordering, output), with the expanded bit
     int32_t *Rp;  // internal id of each result (memory accesses)
     double *qd;
@@ -238,6 +245,7 @@ struct Ctx {
     const __nv_bfloat16 *mlp_w;  // block shared memory copy of the network (or NULL)
     const float *mlp_b;
 };
+using Ctx = CtxT<double>;  // filtered searches and the float64 modes
 
 // Node arrays may be stored in any order (internal ids, chosen for memory locality); results,
 // and ties between equal distances, use the original ids. Sentinel ids outside [0, n) map to
@@ -251,14 +259,16 @@ __device__ __forceinline__ int32_t orig_id(const SearchParams &P, int32_t i) {
 }
 
 // (distance, id) order of two entries whose ids are comparable as they are.
-__device__ __forceinline__ bool pair_lt_raw(double da, int32_t ia, double db, int32_t ib) {
+template <typename T>
+__device__ __forceinline__ bool pair_lt_raw(T da, int32_t ia, T db, int32_t ib) {
     return da < db || (da == db && ia < ib);
 }
 
 
 // ---------------------------------------------------------------------------------------- sorted
 // Entries of the ascending array [0, m) strictly below (d, id).
-__device__ __forceinline__ int count_below(const double *Ad, const int32_t *Ai, int m, double d,
+template <typename T>
+__device__ __forceinline__ int count_below(const T *Ad, const int32_t *Ai, int m, T d,
                                            int32_t id, int lane) {
     int c = 0;
     for (int i = lane; i < m; i += 32) c += pair_lt_raw(Ad[i], Ai[i] & ID_MASK, d, id);
@@ -267,7 +277,8 @@ __device__ __forceinline__ int count_below(const double *Ad, const int32_t *Ai, 
 
 // Same as count_below for a sorted ascending array, by a two-level warp search: 32 splitters, then
 // the chunk that holds the boundary (exact for m <= 1024; falls back to the linear count beyond).
-__device__ __forceinline__ int sorted_rank(const double *Ad, const int32_t *Ai, int m, double d,
+template <typename T>
+__device__ __forceinline__ int sorted_rank(const T *Ad, const int32_t *Ai, int m, T d,
                                            int32_t id, int lane) {
     if (m > 1024) return count_below(Ad, Ai, m, d, id, lane);
     const int step = (m + 31) >> 5;  // entries per chunk
@@ -283,7 +294,8 @@ __device__ __forceinline__ int sorted_rank(const double *Ad, const int32_t *Ai, 
 }
 
 // Entries of the descending array [0, m) strictly above (d, id).
-__device__ __forceinline__ int count_above(const double *Ad, const int32_t *Ai, int m, double d,
+template <typename T>
+__device__ __forceinline__ int count_above(const T *Ad, const int32_t *Ai, int m, T d,
                                            int32_t id, int lane) {
     int c = 0;
     for (int i = lane; i < m; i += 32) c += pair_lt_raw(d, id, Ad[i], Ai[i]);
@@ -291,12 +303,13 @@ __device__ __forceinline__ int count_above(const double *Ad, const int32_t *Ai, 
 }
 
 // Move [pos, m) to [pos + 1, m + 1), highest chunk first (Ap: an optional third array).
-__device__ __forceinline__ void shift_up(double *Ad, int32_t *Ai, int pos, int m, int lane,
+template <typename T>
+__device__ __forceinline__ void shift_up(T *Ad, int32_t *Ai, int pos, int m, int lane,
                                          int32_t *Ap = nullptr) {
     for (int top = m - 1; top >= pos; top -= 32) {
         int i = top - lane;
         bool act = i >= pos;
-        double d = 0.0;
+        T d = T(0);
         int32_t id = 0, ip = 0;
         if (act) {
             d = Ad[i];
@@ -314,12 +327,13 @@ __device__ __forceinline__ void shift_up(double *Ad, int32_t *Ai, int pos, int m
 }
 
 // Move [pos + 1, m) to [pos, m - 1), lowest chunk first (Ap: an optional third array).
-__device__ __forceinline__ void shift_down(double *Ad, int32_t *Ai, int pos, int m, int lane,
+template <typename T>
+__device__ __forceinline__ void shift_down(T *Ad, int32_t *Ai, int pos, int m, int lane,
                                            int32_t *Ap = nullptr) {
     for (int base = pos; base < m - 1; base += 32) {
         int i = base + lane;
         bool act = i < m - 1;
-        double d = 0.0;
+        T d = T(0);
         int32_t id = 0, ip = 0;
         if (act) {
             d = Ad[i + 1];
@@ -593,8 +607,8 @@ __device__ __forceinline__ void dists_bytes(const SearchParams &P, int32_t e, ui
 }
 
 // Distance of one node held uniformly by the warp.
-template <int MODE, bool U8>
-__device__ __forceinline__ double dist_one(const SearchParams &P, Ctx &C, int32_t e) {
+template <int MODE, bool U8, class Cx>
+__device__ __forceinline__ double dist_one(const SearchParams &P, Cx &C, int32_t e) {
     double d = 0.0;
     if (MODE == MODE_BYTES) {
         dists_bytes(P, e, 1u, C.q4, C.lane, d);
@@ -610,7 +624,8 @@ __device__ __forceinline__ double dist_one(const SearchParams &P, Ctx &C, int32_
 // the mask of lanes holding a newly visited neighbour.
 // log2 > 0: the open-addressing hash of the upper layers; log2 == 0: the layer-0 bitmap (one
 // atomicOr per neighbour, no probing), whose marked ids are listed so they can be cleared.
-__device__ __forceinline__ uint32_t mark_chunk(const SearchParams &P, Ctx &C, int32_t e, int log2,
+template <class Cx>
+__device__ __forceinline__ uint32_t mark_chunk(const SearchParams &P, Cx &C, int32_t e, int log2,
                                                int &vis_count) {
     const bool has = e >= 0;
     const uint32_t hmask = __ballot_sync(FULL, has);
@@ -639,7 +654,8 @@ __device__ __forceinline__ uint32_t mark_chunk(const SearchParams &P, Ctx &C, in
 }
 
 // Layer-0 bitmap: mark the entry node.
-__device__ __forceinline__ void bitmap_begin(const SearchParams &P, Ctx &C, int32_t e0) {
+template <class Cx>
+__device__ __forceinline__ void bitmap_begin(const SearchParams &P, Cx &C, int32_t e0) {
     C.vlist_n = 1;
     if (C.lane == 0) {
         atomicOr(C.vbits + (e0 >> 5), 1u << (e0 & 31));
@@ -650,7 +666,8 @@ __device__ __forceinline__ void bitmap_begin(const SearchParams &P, Ctx &C, int3
 
 // Layer-0 bitmap: return every bit this query set to zero (listed words, or the whole bitmap when
 // the list overflowed), so the next query starts from an empty set.
-__device__ __forceinline__ void bitmap_clear(const SearchParams &P, Ctx &C) {
+template <class Cx>
+__device__ __forceinline__ void bitmap_clear(const SearchParams &P, Cx &C) {
     __syncwarp();
     if (C.vlist_n <= P.vlist_cap) {
         for (int i = C.lane; i < C.vlist_n; i += 32) C.vbits[C.vlist[i] >> 5] = 0u;
@@ -663,17 +680,18 @@ __device__ __forceinline__ void bitmap_clear(const SearchParams &P, Ctx &C) {
 }
 
 // Distances of the newly visited neighbours: lane j (bit j of umask) receives its distance in dj.
-template <int MODE, bool U8>
-__device__ __forceinline__ void score_chunk(const SearchParams &P, Ctx &C, int32_t e, uint32_t umask,
-                                            double &dj) {
-    dj = 0.0;
+template <int MODE, bool U8, class Cx>
+__device__ __forceinline__ void score_chunk(const SearchParams &P, Cx &C, int32_t e, uint32_t umask,
+                                            typename Cx::dist_t &dj) {
+    double d = 0.0;
     if (MODE == MODE_BYTES) {
-        dists_bytes(P, e, umask, C.q4, C.lane, dj);
+        dists_bytes(P, e, umask, C.q4, C.lane, d);
     } else if (MODE == MODE_EXACT) {
-        dists_exact_f32<U8>(P, e, umask, C.qf, C.lane, dj);
+        dists_exact_f32<U8>(P, e, umask, C.qf, C.lane, d);
     } else if ((umask >> C.lane) & 1u) {
-        dj = dist_seq_f64<U8>(P, e, C.qd);
+        d = dist_seq_f64<U8>(P, e, C.qd);
     }
+    dj = typename Cx::dist_t(d);
 }
 
 // Byte rows of at most 128 bytes starting on 16-byte boundaries (dim a multiple of 16): every lane
@@ -682,15 +700,18 @@ __device__ __forceinline__ void score_chunk(const SearchParams &P, Ctx &C, int32
 // arrive in one memory round trip. Rows of neighbours found already visited are dropped unscored and
 // uncounted. Each lane then sums its own row against the query (shared-memory broadcast reads):
 // integer arithmetic, so the value equals dists_bytes' bit for bit.
-__device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, Ctx &C, int32_t e,
-                                                         int log2, int &vis_count, double &dj) {
+template <class Cx>
+__device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, Cx &C, int32_t e,
+                                                         int log2, int &vis_count,
+                                                         typename Cx::dist_t &dj) {
+    using D = typename Cx::dist_t;
     const int v4 = P.dim >> 4;
     const uint4 *row = reinterpret_cast<const uint4 *>(P.rows8 + int64_t(e < 0 ? 0 : e) * P.dim);
     uint4 x[8];
 #pragma unroll
     for (int t = 0; t < 8; t++) x[t] = (e >= 0 && t < v4) ? __ldg(row + t) : make_uint4(0u, 0u, 0u, 0u);
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
-    dj = 0.0;
+    dj = D(0);
     if ((um >> C.lane) & 1u) {
         const uint4 *qv = reinterpret_cast<const uint4 *>(C.q4);
         uint32_t acc = 0u;
@@ -709,7 +730,7 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, 
                     acc = __dp4a(d, d, acc);
                 }
             }
-            dj = double(acc);
+            dj = D(acc);
         } else {
 #pragma unroll
             for (int t = 0; t < 8; t++) {
@@ -721,16 +742,16 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, 
                     acc = __dp4a(x[t].w, q.w, acc);
                 }
             }
-            dj = -double(acc);
+            dj = -D(acc);
         }
     }
     return um;
 }
 
 // Mark a chunk visited and score its new neighbours (lane j of the returned mask gets dj).
-template <int MODE, bool U8>
-__device__ __forceinline__ uint32_t mark_and_score(const SearchParams &P, Ctx &C, int32_t e, int log2,
-                                                   int &vis_count, double &dj) {
+template <int MODE, bool U8, class Cx>
+__device__ __forceinline__ uint32_t mark_and_score(const SearchParams &P, Cx &C, int32_t e, int log2,
+                                                   int &vis_count, typename Cx::dist_t &dj) {
     if (MODE == MODE_BYTES && HB_LANE_ROWS && C.lane_rows)
         return mark_score_lane_rows(P, C, e, log2, vis_count, dj);
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
@@ -761,7 +782,8 @@ __device__ __forceinline__ int32_t first_link(const int32_t *nb, int stride, int
 // ------------------------------------------------------------------------ learned early termination
 // Warp matvec of the 12 -> 64 -> 64 -> 1 ReLU network: BF16 weights, FP32 accumulation. Every lane
 // holds the same (uniform) features; lane j computes hidden units j and j + 32.
-__device__ __forceinline__ float mlp_eval(const Ctx &C, const float (&raw)[STOP_FEATURES]) {
+template <class Cx>
+__device__ __forceinline__ float mlp_eval(const Cx &C, const float (&raw)[STOP_FEATURES]) {
     const int lane = C.lane;
     const __nv_bfloat162 *w1 = reinterpret_cast<const __nv_bfloat162 *>(C.mlp_w);  // [i][l]
     const __nv_bfloat162 *w2 = w1 + STOP_FEATURES * 32;                              // [i][l]
@@ -812,19 +834,20 @@ struct StopState {
 };
 
 // At a checkpoint: features, optional trace row, optional network decision (true = stop).
-__device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, StopState &S, int r,
-                                                int scan, double W) {
+template <class Cx>
+__device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Cx &C, StopState &S, int r,
+                                                int scan, typename Cx::dist_t W) {
     const int lane = C.lane;
     const int kk = min(r, P.k);
     const float dk = log1pf(float(C.Rd[kk - 1]));
     const float d1 = log1pf(float(C.Rd[0]));
     // Frontier: distance of the next candidate the search would expand (the worst if none).
-    double dn = W;
+    double dn = double(W);
     for (int b = scan; b < r; b += 32) {
         const int i = b + lane;
         const uint32_t m = __ballot_sync(FULL, i < r && !(C.Ri[i] & EXP_BIT));
         if (m) {
-            dn = C.Rd[b + __ffs(m) - 1];
+            dn = double(C.Rd[b + __ffs(m) - 1]);
             break;
         }
     }
@@ -853,7 +876,7 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, S
         }
         if (lane < P.trace_k)
             P.trace_dk[(int64_t(C.q) * P.trace_cap + S.cp) * P.trace_k + lane] =
-                lane < r ? C.Rd[lane] : INFINITY;
+                lane < r ? double(C.Rd[lane]) : double(INFINITY);
     }
     S.cp++;
     S.dk_prev2 = S.dk_prev;
@@ -885,12 +908,14 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Ctx &C, S
 // only if the worst distance did not drop, and gains the unexpanded evicted entries that tie the
 // final worst, pushed in descending (distance, id) order as the evictions would have pushed them.
 // churn (a stop feature) counts admissions that entered the first k at their insertion time.
-__device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32_t e, int32_t eo,
-                                            double dj, uint32_t um, int ef, int &r, double &W,
-                                            int &scan, int &tn, int &churn) {
+template <class Cx>
+__device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_t e, int32_t eo,
+                                            typename Cx::dist_t dj, uint32_t um, int ef, int &r,
+                                            typename Cx::dist_t &W, int &scan, int &tn, int &churn) {
+    using D = typename Cx::dist_t;
     const int lane = C.lane;
     const int r0 = r;
-    const double W0 = W;
+    const D W0 = W;
     const uint32_t cm = __ballot_sync(FULL, ((um >> lane) & 1u) && (r0 < ef || dj < W0));
     if (!cm) return;
     const bool inc = (cm >> lane) & 1u;
@@ -912,7 +937,7 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32
     for (uint32_t m = cm; m;) {
         const int i = __ffs(m) - 1;
         m &= m - 1;
-        const double di = __shfl_sync(FULL, dj, i);
+        const D di = __shfl_sync(FULL, dj, i);
         prev_le += (i < lane && di <= dj);
     }
     const bool adm = inc && lo + n_eq + prev_le < ef;
@@ -922,7 +947,7 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32
     for (uint32_t m = A; m;) {
         const int i = __ffs(m) - 1;
         m &= m - 1;
-        const double di = __shfl_sync(FULL, dj, i);
+        const D di = __shfl_sync(FULL, dj, i);
         const int32_t ii = __shfl_sync(FULL, eo, i);
         const bool lt = di < dj || (di == dj && ii < eo);
         rank_a += lt;
@@ -939,7 +964,7 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32
     for (int top = r0 - 1; top >= pmin; top -= 64) {
         const int p1 = top - lane, p2 = top - 32 - lane;
         const bool a1 = p1 >= pmin, a2 = p2 >= pmin;
-        double d1 = 0.0, d2 = 0.0;
+        D d1 = D(0), d2 = D(0);
         int32_t i1 = 0, i2 = 0, q1 = 0, q2 = 0;
         if (a1) {
             d1 = C.Rd[p1];
@@ -981,7 +1006,7 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32
     int rn = r0 + __popc(A);
     if (rn > ef) {
         const int nev = rn - ef;  // at most 32
-        const double wf = C.Rd[ef - 1];
+        const D wf = C.Rd[ef - 1];
         if (r0 == ef && wf != W0) tn = 0;  // the worst dropped: earlier ties are too far now
         bool push = false;
         int32_t pid = 0;
@@ -1005,8 +1030,9 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Ctx &C, int32
     scan = min(scan, fmin);
 }
 
-template <int MODE, bool U8>
-__device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, int log2, int &r) {
+template <int MODE, bool U8, class Cx>
+__device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, int log2, int &r) {
+    using D = typename Cx::dist_t;
     const int lane = C.lane;
     if (layer > 0 || (HB_L0_HASH && log2 > 0)) {
         vis_clear(C.vis, log2, lane);
@@ -1018,7 +1044,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
     }
     int vis_count = 1;
     const int vis_lim = log2 > 0 ? ((1 << log2) >> 2) * 3 : 0x7fffffff;
-    double W = C.Rd[r - 1];
+    D W = C.Rd[r - 1];
     int scan = 0;  // every result before `scan` is expanded
     int tn = 0;    // tie stack depth
     const bool track = layer == 0 && (P.trace_feat != nullptr || C.mlp_w != nullptr);
@@ -1062,7 +1088,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
 #endif
             HB_PROF(2);
             HB_PROF(3);
-            double dj;
+            D dj;
             const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
 #ifdef HB_PROFILE
             if (__shfl_sync(FULL, dj, 0) == -12345.0) C.status |= 64;  // consume before timing
@@ -1078,7 +1104,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
             while (am) {
                 const int j = __ffs(am) - 1;
                 am &= am - 1;
-                const double d = __shfl_sync(FULL, dj, j);
+                const D d = __shfl_sync(FULL, dj, j);
                 const int32_t id = __shfl_sync(FULL, eo, j);
                 const int32_t pid = __shfl_sync(FULL, e, j);
                 if (!(r < ef || d < W)) continue;  // uniform
@@ -1095,7 +1121,7 @@ __device__ void layer_search(const SearchParams &P, Ctx &C, int layer, int ef, i
                 if (pos < scan) scan = pos;
                 if (r > ef) {  // evict the maximum (d, id)
                     r = ef;
-                    const double ed = C.Rd[ef];
+                    const D ed = C.Rd[ef];
                     const int32_t ei = C.Ri[ef];
                     if (ed == C.Rd[ef - 1]) {
                         if (!(ei & EXP_BIT)) {  // still a candidate, tied with the worst
@@ -1347,7 +1373,8 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
 // ------------------------------------------------------------------------------ rerank epilogue
 // numba_engine._rerank_batch (:506-530): exact float64 distances from the float32 query to the
 // first m beam entries, best k by (distance, id).
-__device__ int rerank_epilogue(const SearchParams &P, Ctx &C, int m) {
+template <class Cx>
+__device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m) {
     const int lane = C.lane;
     const int k = P.k;
     int a = 0;
@@ -1387,9 +1414,10 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
     const bool two_ids = P.node_ids != nullptr;
     const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids);
     unsigned char *p = smem + size_t(warp) * wb;
-    Ctx C;
+    using D = std::conditional_t<(MODE == MODE_BYTES && !FILT), float, double>;
+    CtxT<D> C;
     C.lane = lane;
-    C.Rd = reinterpret_cast<double *>(p);
+    C.Rd = reinterpret_cast<D *>(p);  // 8 bytes a slot are reserved either way
     p += al16(size_t(result_slots(P.ef_cap)) * 8);
     C.Ri = reinterpret_cast<int32_t *>(p);
     p += al16(size_t(result_slots(P.ef_cap)) * 4);
@@ -1489,7 +1517,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
         int r = 1;
         for (int layer = P.max_level; layer > 0 && !C.status; layer--) {
             if (lane == 0) {
-                C.Rd[0] = d0;
+                C.Rd[0] = D(d0);
                 C.Ri[0] = o0;
                 C.Rp[0] = e0;
             }
@@ -1503,11 +1531,11 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
         }
         const int ef0 = max(__ldg(P.ef + q), P.k_search);
         if (!C.status) {
-            if (FILT) {
+            if constexpr (FILT) {
                 layer0_filtered<MODE, U8>(P, C, ef0, P.vis_log2, d0, e0, o0, r);
             } else {
                 if (lane == 0) {
-                    C.Rd[0] = d0;
+                    C.Rd[0] = D(d0);
                     C.Ri[0] = o0;
                     C.Rp[0] = e0;
                 }
@@ -1540,7 +1568,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
         } else {
             for (int i = lane; i < k; i += 32) {
                 oi[i] = i < r ? int64_t(C.Ri[i] & ID_MASK) : -1;
-                od[i] = i < r ? C.Rd[i] : INFINITY;
+                od[i] = i < r ? double(C.Rd[i]) : double(INFINITY);
             }
         }
 #ifdef HB_PROFILE
