@@ -76,3 +76,28 @@ def test_upload_rejects_null_arguments(lib) -> None:
     buf = (ctypes.c_float * 8)()
     assert lib.hnsw_b200_upload_queries(None, None, 0, 1, ctypes.byref(st),
                                         ctypes.addressof(buf) + 4, None) == -1
+
+
+def test_concurrent_callers_each_get_their_own_statistics(lib) -> None:
+    """The host pool runs one batch at a time: callers on several threads (ctypes releases the
+    GIL) each get the statistics of their own batch."""
+    import threading
+
+    rng = np.random.default_rng(9)
+    batches = [rng.integers(0, 256, 300_000).astype(np.float32) for _ in range(6)]
+    batches[2] = batches[2] + 0.5  # not integer
+    batches[4][77] = np.inf        # not finite
+    want = [(bool(np.isfinite(b).all()), bool(np.array_equal(b, np.rint(b)))) for b in batches]
+    got: list = [None] * len(batches)
+
+    def run(i: int) -> None:
+        for _ in range(20):
+            st = _scan(lib, batches[i], 8)
+            got[i] = (bool(st.finite), bool(st.integer) if st.finite else want[i][1])
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(len(batches))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert got == want
