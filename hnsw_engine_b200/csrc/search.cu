@@ -207,9 +207,9 @@ __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filt
     return b;
 }
 
-// D: the type of the result distances Rd. Unfiltered byte searches use float -- their distances
-// are integers of magnitude at most 128 * 255^2 < 2^24, exact in float32, so order and ties are
-// unchanged -- halving the result list's shuffles and shared-memory traffic and keeping its
+// D: the type of the result and candidate distances (Rd, Sd, spd). Byte searches use float --
+// their distances are integers of magnitude at most 128 * 255^2 < 2^24, exact in float32, so order
+// and ties are unchanged -- halving the lists' shuffles and memory traffic and keeping their
 // compares off the FP64 pipe. Every other search uses double.
 template <typename D>
 struct CtxT {
@@ -221,7 +221,7 @@ struct CtxT {
     double *qd;
     float *qf;
     uint32_t *q4;  // query bytes, four per word (byte mode)
-    double *Sd;
+    D *Sd;
     int32_t *Si;  // candidates: original ids
     int32_t *Sp;  // candidates: internal ids (the same array as Si unless the order differs)
     double *Ad;
@@ -231,7 +231,7 @@ struct CtxT {
     int32_t *vlist;
     int32_t vlist_n;  // ids appended to vlist (may exceed the capacity: then clear everything)
     int32_t *ties;
-    double *spd;
+    D *spd;
     int32_t *spi;
     int32_t *spp;
     long long ndist, nhops;  // uniform across the warp
@@ -1154,14 +1154,17 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
 }
 
 // -------------------------------------------------------------------- filtered candidate storage
-struct Cands {
+template <typename D>
+struct CandsT {
     int s;        // entries in S (descending: S[s-1] is the minimum)
     int g;        // entries in the global spill G
-    double gd;    // minimum (d, id) of G when g > 0
+    D gd;         // minimum (d, id) of G when g > 0
     int32_t gi;
 };
 
-__device__ __forceinline__ void spill_push(const SearchParams &P, Ctx &C, Cands &K, double d,
+template <class Cx>
+__device__ __forceinline__ void spill_push(const SearchParams &P, Cx &C,
+                                           CandsT<typename Cx::dist_t> &K, typename Cx::dist_t d,
                                            int32_t id, int32_t ip) {
     if (K.g < P.spill_cap) {
         if (C.lane == 0) {
@@ -1176,8 +1179,11 @@ __device__ __forceinline__ void spill_push(const SearchParams &P, Ctx &C, Cands 
 }
 
 // id: original id (ordering); ip: internal id (expansion).
-__device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &K, double d,
+template <class Cx>
+__device__ __forceinline__ void cand_push(const SearchParams &P, Cx &C,
+                                          CandsT<typename Cx::dist_t> &K, typename Cx::dist_t d,
                                           int32_t id, int32_t ip) {
+    using D = typename Cx::dist_t;
     int32_t *sp = C.Sp != C.Si ? C.Sp : nullptr;
     if (K.g > 0 && !pair_lt_raw(d, id, K.gd, K.gi)) {  // not below the spill minimum
         spill_push(P, C, K, d, id, ip);
@@ -1193,7 +1199,7 @@ __device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &
     __syncwarp();
     K.s++;
     if (K.s > P.s_cap) {  // move the maximum to the spill; it becomes the spill minimum
-        const double md = C.Sd[0];
+        const D md = C.Sd[0];
         const int32_t mi = C.Si[0];
         const int32_t mp = sp ? sp[0] : mi;
         shift_down(C.Sd, C.Si, 0, K.s, C.lane, sp);
@@ -1206,14 +1212,17 @@ __device__ __forceinline__ void cand_push(const SearchParams &P, Ctx &C, Cands &
 
 // Refill the empty S with the smallest spill entries (at most s_cap / 2), dropping entries that
 // can no longer be expanded (distance above the worst of full results).
-__device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune, double Wp) {
+template <class Cx>
+__device__ void cand_refill(const SearchParams &P, Cx &C, CandsT<typename Cx::dist_t> &K, bool prune,
+                            typename Cx::dist_t Wp) {
+    using D = typename Cx::dist_t;
     const int lane = C.lane;
     const int B = max(1, P.s_cap / 2);
     int32_t *sp = C.Sp != C.Si ? C.Sp : nullptr;
     int s = 0;
     for (int base = 0; base < K.g; base += 32) {
         const int i = base + lane;
-        double d = 0.0;
+        D d = D(0);
         int32_t id = 0, ip = 0;
         bool v = i < K.g;
         if (v) {
@@ -1226,7 +1235,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
         while (cm) {
             const int j = __ffs(cm) - 1;
             cm &= cm - 1;
-            const double xd = __shfl_sync(FULL, d, j);
+            const D xd = __shfl_sync(FULL, d, j);
             const int32_t xi = __shfl_sync(FULL, id, j);
             const int32_t xp = sp ? __shfl_sync(FULL, ip, j) : xi;
             if (!(s < B || pair_lt_raw(xd, xi, C.Sd[0], C.Si[0]))) continue;
@@ -1247,14 +1256,14 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
         }
     }
     // Compact the spill: keep entries not selected (above S's maximum) and not pruned.
-    const double td = s > 0 ? C.Sd[0] : -INFINITY;
+    const D td = s > 0 ? C.Sd[0] : -D(INFINITY);
     const int32_t ti = s > 0 ? C.Si[0] : -1;
     int w = 0;
-    double md = INFINITY;
+    D md = D(INFINITY);
     int32_t mi = 0x7fffffff;
     for (int base = 0; base < K.g; base += 32) {
         const int i = base + lane;
-        double d = 0.0;
+        D d = D(0);
         int32_t id = 0, ip = 0;
         bool keep = false;
         if (i < K.g) {
@@ -1280,7 +1289,7 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        const double od = __shfl_xor_sync(FULL, md, o);
+        const D od = __shfl_xor_sync(FULL, md, o);
         const int32_t oi = __shfl_xor_sync(FULL, mi, o);
         if (pair_lt_raw(od, oi, md, mi)) {
             md = od;
@@ -1297,35 +1306,36 @@ __device__ void cand_refill(const SearchParams &P, Ctx &C, Cands &K, bool prune,
 // numba_engine._search_layer0_filtered (:151-198): results hold allowed nodes only, the worst of
 // an empty result list is +inf, and the search stops only when the results are full and the
 // closest candidate is strictly farther than the worst.
-template <int MODE, bool U8>
-__device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2, double d0,
+template <int MODE, bool U8, class Cx>
+__device__ void layer0_filtered(const SearchParams &P, Cx &C, int ef, int log2, double d0,
                                 int32_t e0, int32_t o0, int &r) {
+    using D = typename Cx::dist_t;
     const int lane = C.lane;
     log2 = 0;  // bitmap
     bitmap_begin(P, C, e0);
     if (lane == 0) {  // candidates hold internal ids; results hold both
-        C.Sd[0] = d0;
+        C.Sd[0] = D(d0);
         C.Si[0] = o0;
         C.Sp[0] = e0;
         if (is_allowed(P.allowed, e0)) {
-            C.Rd[0] = d0;
+            C.Rd[0] = D(d0);
             C.Ri[0] = o0;
             C.Rp[0] = e0;
         }
     }
     __syncwarp();
     r = is_allowed(P.allowed, e0) ? 1 : 0;
-    Cands K{1, 0, INFINITY, 0x7fffffff};
+    CandsT<D> K{1, 0, D(INFINITY), 0x7fffffff};
     int vis_count = 1;
     const int vis_lim = 0x7fffffff;
-    double W = r > 0 ? C.Rd[r - 1] : INFINITY;
+    D W = r > 0 ? C.Rd[r - 1] : D(INFINITY);
     for (;;) {
         if (K.s == 0) {
             if (K.g == 0) break;
             cand_refill(P, C, K, r == ef, W);
             if (K.s == 0) break;
         }
-        const double dc = C.Sd[K.s - 1];
+        const D dc = C.Sd[K.s - 1];
         const int32_t c = C.Sp[K.s - 1];
         K.s--;
         if (r == ef && dc > W) break;
@@ -1336,14 +1346,14 @@ __device__ void layer0_filtered(const SearchParams &P, Ctx &C, int ef, int log2,
             const int32_t e = base == 0 ? first_link(nb, P.links0_stride, cnt, lane)
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
             const int32_t eo = e >= 0 ? orig_id(P, e) : -1;
-            double dj;
+            D dj;
             const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
                 const int j = __ffs(am) - 1;
                 am &= am - 1;
-                const double d = __shfl_sync(FULL, dj, j);
+                const D d = __shfl_sync(FULL, dj, j);
                 const int32_t id = __shfl_sync(FULL, e, j);
                 const int32_t ido = __shfl_sync(FULL, eo, j);
                 if (!(r < ef || d < W)) continue;
@@ -1414,7 +1424,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
     const bool two_ids = P.node_ids != nullptr;
     const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids);
     unsigned char *p = smem + size_t(warp) * wb;
-    using D = std::conditional_t<(MODE == MODE_BYTES && !FILT), float, double>;
+    using D = std::conditional_t<MODE == MODE_BYTES, float, double>;
     CtxT<D> C;
     C.lane = lane;
     C.Rd = reinterpret_cast<D *>(p);  // 8 bytes a slot are reserved either way
@@ -1436,7 +1446,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
     C.Si = nullptr;
     C.Sp = nullptr;
     if (FILT) {
-        C.Sd = reinterpret_cast<double *>(p);
+        C.Sd = reinterpret_cast<D *>(p);
         p += al16(size_t(P.s_cap + 1) * 8);
         C.Si = reinterpret_cast<int32_t *>(p);
         p += al16(size_t(P.s_cap + 1) * 4);
@@ -1466,7 +1476,8 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
     C.vlist = P.vlist + slot * P.vlist_cap;
     C.vlist_n = 0;
     C.ties = P.ties + slot * P.tie_cap;
-    C.spd = FILT ? P.spill_d + slot * P.spill_cap : nullptr;
+    // byte searches keep float candidates: the first half of each slot of the double spill
+    C.spd = FILT ? reinterpret_cast<D *>(P.spill_d + slot * P.spill_cap) : nullptr;
     C.spi = FILT ? P.spill_i + slot * P.spill_cap : nullptr;
     C.spp = FILT ? (two_ids ? P.spill_p + slot * P.spill_cap : C.spi) : nullptr;
     C.lane_rows = P.lane_rows && (P.dim & 15) == 0 && P.dim <= 128;
