@@ -1,14 +1,14 @@
-// Upload of a float32 query batch: the caller's thread copies it to the GPU (a pageable
-// cudaMemcpyAsync, which stages through the driver's own pinned buffers) while a small persistent
-// pool of host threads reads the same values and gathers what the choice of distance arithmetic
-// needs: every value finite, every value an integer, minimum and maximum. The choice is then made
-// on the host, so nothing reads the batch back from the GPU before the search launch. For
-// contiguous float32 batches this replaces the host validator's NaN/inf pass (the reference's
-// _validation.py:30-35, "contains NaN or infinite values") and the float32 cast of
-// metrics.py:49-53, a copy for float32 rows.
+// Upload of a float32 query batch. A small persistent pool of host threads reads the values once
+// and gathers what the choice of distance arithmetic needs: every value finite, every value an
+// integer, minimum and maximum. The choice is then made on the host, so nothing reads the batch
+// back from the GPU before the search launch. For contiguous float32 batches this replaces the host
+// validator's NaN/inf pass (the reference's _validation.py:30-35, "contains NaN or infinite
+// values") and the float32 cast of metrics.py:49-53, a copy for float32 rows.
 //
-// With a page-locked staging buffer the pool threads also copy the rows into it, with streaming
-// (non-temporal) stores, and one asynchronous DMA follows. Measured on the B200 hosts (16 vCPUs),
+// The batch reaches the GPU one of two ways. Without a staging buffer, the calling thread issues a
+// pageable cudaMemcpyAsync during the read (the driver stages it through its own pinned buffers).
+// With a page-locked staging buffer, the pool threads copy the rows into it as they read them,
+// with streaming (non-temporal) stores, and one asynchronous DMA follows. Measured on the B200 hosts (16 vCPUs),
 // 5 MB: the pageable copy takes 0.30 ms; staging by 4 threads plus the DMA 0.22 ms with streaming
 // stores, but 0.86 ms with ordinary ones -- a DMA read of lines still dirty in other cores' caches
 // is slow there.
@@ -20,6 +20,7 @@
 #include <cstring>
 #include <functional>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -38,15 +39,23 @@ namespace {
 
 // Workers wait on a generation counter; run() hands every worker the same job (worker w runs part
 // w - 1 when w <= parts), runs `caller` on the calling thread meanwhile, and returns when all are
-// done. One run at a time (run_mutex_). The pool is never destroyed (its threads end with the
-// process); a forked child builds its own.
+// done. One run at a time (run_mutex_). The pool is allocated once and never destroyed (its
+// detached threads end with the process, and always find it alive); a forked child builds its
+// own. Workers start one at a time; if the system refuses a thread, the pool keeps those it has.
 class HostPool {
    public:
-    explicit HostPool(int workers) {
-        for (int i = 0; i < workers; ++i) threads_.emplace_back([this, i] { loop(i + 1); });
-        for (auto &t : threads_) t.detach();
+    void start(int workers) {
+        for (int i = 0; i < workers; ++i) {
+            try {
+                std::thread t([this, i] { loop(i + 1); });
+                t.detach();
+            } catch (...) {
+                break;
+            }
+            ++workers_;
+        }
     }
-    int workers() const { return int(threads_.size()); }
+    int workers() const { return workers_; }
 
     void run(int parts, const std::function<void(int)> &fn, const std::function<void()> &caller) {
         std::lock_guard<std::mutex> serial(run_mutex_);
@@ -54,7 +63,7 @@ class HostPool {
             std::lock_guard<std::mutex> lk(m_);
             job_ = &fn;
             parts_ = parts;
-            pending_ = int(threads_.size());
+            pending_ = workers_;
             ++gen_;
         }
         wake_.notify_all();
@@ -79,7 +88,7 @@ class HostPool {
         }
     }
 
-    std::vector<std::thread> threads_;
+    int workers_ = 0;
     std::mutex run_mutex_, m_;
     std::condition_variable wake_, done_;
     const std::function<void(int)> *job_ = nullptr;
@@ -87,17 +96,21 @@ class HostPool {
     uint64_t gen_ = 0;
 };
 
-HostPool &pool() {
+// The process's pool, or nullptr if none could be made (the caller then works alone).
+HostPool *pool() noexcept {
     static std::mutex m;
     static HostPool *p = nullptr;
     static pid_t owner = 0;
     std::lock_guard<std::mutex> lk(m);
     if (p == nullptr || owner != getpid()) {
         const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
-        p = new HostPool(int(std::min(hw - 1, 16u)));
+        HostPool *fresh = new (std::nothrow) HostPool();
+        if (fresh == nullptr) return nullptr;
+        fresh->start(int(std::min(hw - 1, 16u)));
+        p = fresh;
         owner = getpid();
     }
-    return *p;
+    return p;
 }
 
 struct Part {
@@ -176,20 +189,21 @@ extern "C" int hnsw_b200_upload_queries(const float *src, float *dst, int64_t co
     // at least 64K values (256 KB) per part: below that a wake-up costs more than the scan
     constexpr int64_t MIN_PART = 65536;
     int parts = int(std::min<int64_t>(std::max(1, threads), (count + MIN_PART - 1) / MIN_PART));
+    HostPool *hp = parts > 1 ? pool() : nullptr;
+    if (hp == nullptr || hp->workers() < 2) parts = 1;
     std::vector<Part> res;
     if (parts <= 1) {
         copy();
         res.push_back(scan(src, stage, 0, count));
     } else {
-        HostPool &p = pool();
-        parts = std::min(parts, p.workers());
+        parts = std::min(parts, hp->workers());
         res.resize(size_t(parts));
         const int64_t per = ((count + parts - 1) / parts + 15) / 16 * 16;  // aligned part starts
         const std::function<void(int)> job = [&](int i) {
             const int64_t b = std::min(count, int64_t(i) * per);
             res[size_t(i)] = scan(src, stage, b, std::min(count, b + per));
         };
-        p.run(parts, job, stage ? nothing : copy);
+        hp->run(parts, job, stage ? nothing : copy);
     }
     if (stage != nullptr && count > 0)  // one asynchronous DMA of the staged rows
         copy_err = cudaMemcpyAsync(dst, stage, size_t(count) * sizeof(float),
