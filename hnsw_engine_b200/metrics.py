@@ -1,4 +1,4 @@
-"""Recall judge: the reference's tie-aware recall@k (``src/hnsw_engine/bench/metrics.py:13-51``).
+"""Recall measure: the reference's tie-aware recall@k (``src/hnsw_engine/bench/metrics.py:13-51``).
 
 A returned id counts when it is a valid id (not ``-1``), not a repeat within the row, and its exact
 distance is at most the exact k-th neighbour distance plus ``1e-9 * max(1, |kth|)``: equally close

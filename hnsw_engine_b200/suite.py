@@ -2,7 +2,7 @@
 
 The headline metric is ``bench.py``'s; this suite measures the other configurations of the same
 engine on one GPU with device-resident inputs (CUDA events, median of repeated launches) and the
-recall judge against the tensor-core exact k-NN:
+recall measured against the tensor-core exact k-NN:
 
 * ``sweep``: plain search at a list of efSearch values (10K and 1M mixture, 1M Student-t);
 * ``modes``: the same search with byte rows, exact float32 rows and float64 rows (1M mixture);
