@@ -8,10 +8,9 @@
 //   _distance                numba_engine.py:57-70                     -> dist_seq_f64 / dists_exact_f32
 //   _rerank_batch            numba_engine.py:506-530                   -> rerank_epilogue
 // and the canonical rules of the reference project's own docs/DESIGN.md, section 5 (rules 4, 5,
-// 9): candidates pop in
-// ascending (distance, id); a neighbour is admitted iff the results hold fewer than ef entries or
-// its distance is strictly below the running worst, neighbours taken in stored link order; the
-// worst result (maximum (distance, id)) is evicted.
+// 9): candidates pop in ascending (distance, id); a neighbour is admitted iff the results hold
+// fewer than ef entries or its distance is strictly below the running worst, neighbours taken in
+// stored link order; the worst result (maximum (distance, id)) is evicted.
 //
 // Data structures (per query, one warp):
 //  * results R: a sorted (distance, id) array in shared memory with an "expanded" bit per entry.
