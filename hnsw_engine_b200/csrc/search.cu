@@ -2023,38 +2023,29 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
 }  // extern "C"
 
 // =========================================================================== fixed-scratch search
-// Some callers cannot allocate device memory at all: code running inside a CUDA-graph-captured
-// region or a real-time serving loop where an allocation would stall or be forbidden, plugins whose
-// host owns every device allocation through its own pool, and processes started under a hard device
-// memory budget. For them hnsw_b200_search_noalloc runs the same search kernel with all of its
-// working memory carved out of one fixed array that is part of the library image. The array is
-// HB_NOALLOC_BYTES (32 MiB) of device memory that every GPU which loads this library keeps until the
-// process exits, whether or not the entry point is used.
+// Some callers cannot allocate device memory at all: real-time serving loops where an allocation
+// would stall the loop, plugins whose host owns every device allocation through its own pool, and
+// processes started under a hard device-memory budget. For them hnsw_b200_search_noalloc runs the
+// same search kernel with all of its working memory carved out of one fixed array that is part of
+// the library image. The array is HB_NOALLOC_BYTES (32 MiB) of device memory that every GPU which
+// loads this library keeps until the process exits, whether or not the entry point is used. The
+// call waits for its stream once before returning, to read how many queries overflowed.
 namespace hb {
 
 constexpr size_t HB_NOALLOC_BYTES = size_t(32) << 20;
 constexpr int32_t HB_NOALLOC_MAX_NQ = 1 << 20;  // per-query status words live in the array too
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HB_NOALLOC_BYTES];
 
-// Device address of g_noalloc_scratch, looked up once per device (the host-side symbol is only a
-// handle, not an address a kernel may use).
-std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[128] = {nullptr};
-
+// Device address of g_noalloc_scratch on the current device. The host-side symbol is only a
+// handle, not an address a kernel may use. It is looked up on every call rather than cached, so a
+// context that was destroyed and recreated (cudaDeviceReset) never leaves a stale pointer behind.
 int noalloc_scratch(void **out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
-        return fail(HNSW_B200_ECUDA, "search_noalloc: no current CUDA device");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(HNSW_B200_ECUDA, std::string("search_noalloc: cudaGetSymbolAddress failed: ") +
-                                             cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(HNSW_B200_ECUDA, std::string("search_noalloc: cudaGetSymbolAddress failed: ") +
+                                         cudaGetErrorString(e));
+    *out = p;
     return 0;
 }
 
@@ -2072,6 +2063,8 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     if (g.max_level > 0 && (!g.links_up || !g.count_up || g.rows <= 0))
         return fail(HNSW_B200_EINVAL, "search_noalloc: upper layers need links_up and count_up");
     if (a->allowed) return fail(HNSW_B200_EINVAL, "search_noalloc: filtered search needs hnsw_b200_search");
+    if (a->priority)
+        return fail(HNSW_B200_EINVAL, "search_noalloc: no start order (priority must be NULL)");
     if (a->nq < 0) return fail(HNSW_B200_EINVAL, "nq out of range");
     if (a->nq > HB_NOALLOC_MAX_NQ)
         return fail(HNSW_B200_EINVAL, "search_noalloc: at most " + std::to_string(HB_NOALLOC_MAX_NQ) +
@@ -2100,17 +2093,9 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     const bool use_mlp = a->stop_mlp != nullptr;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (smem_block > 227 * 1024) return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory");
-    int bps = 0;
-    if (int rc = occupancy(mode, u8, false, smem_block, &bps)) return rc;
-    if (bps < 1) return fail(HNSW_B200_EINVAL, "search kernel cannot be resident");
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-
     // Carve the fixed array: counters, per-query status, then per warp slot the layer-0 bitmap, its
     // list of marked ids, the upper-layer hash and the tie stack. The slot count is whatever fits.
-    void *base = nullptr;
-    if (int rc = noalloc_scratch(&base)) return rc;
+    // Requests that cannot fit are rejected here, before any CUDA call.
     const int32_t nq = int32_t(a->nq);
     const int64_t vbits_stride = ((g.n + 31) / 32 + 3) / 4 * 4;
     const int vlist_cap = int(std::min<int64_t>(65536, std::max<int64_t>(256, g.n / 256)));
@@ -2123,6 +2108,14 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
         return fail(HNSW_B200_EINVAL, "search_noalloc: graph of " + std::to_string(g.n) +
                                           " nodes needs more than the fixed " +
                                           std::to_string(HB_NOALLOC_BYTES >> 20) + " MiB scratch");
+    int bps = 0;
+    if (int rc = occupancy(mode, u8, false, smem_block, &bps)) return rc;
+    if (bps < 1) return fail(HNSW_B200_EINVAL, "search kernel cannot be resident");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    void *base = nullptr;
+    if (int rc = noalloc_scratch(&base)) return rc;
     const int64_t slot_fit = int64_t((HB_NOALLOC_BYTES - head) / per_slot) / WPB * WPB;
     const int blocks = int(std::min<int64_t>(std::min<int64_t>(int64_t(sms) * bps, slot_fit / WPB),
                                              (nq + WPB - 1) / WPB));

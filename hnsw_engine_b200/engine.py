@@ -15,6 +15,7 @@ over the dimensions, which is the reference's own arithmetic (``_distance``, num
 from __future__ import annotations
 
 import ctypes
+import warnings
 from typing import Any
 
 import numpy as np
@@ -55,7 +56,14 @@ def to_device(a: Any, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
             return a.to(device=device, non_blocking=True)
         return a.to(device=device, dtype=dtype).contiguous()
     arr = np.ascontiguousarray(a)
-    t = torch.from_numpy(arr)
+    if arr.flags.writeable:
+        t = torch.from_numpy(arr)
+    else:
+        # Read-only source (an mmap of a native .npy): the tensor is only read, by the copy below,
+        # so torch's warning about writes through non-writable memory does not apply.
+        with warnings.catch_warnings():
+            warnings.filterwarnings("ignore", message="The given NumPy array is not writable")
+            t = torch.from_numpy(arr)
     if t.dtype != dtype:
         t = t.to(dtype)
     return t.to(device, non_blocking=False).contiguous()
@@ -370,19 +378,23 @@ class DeviceGraph:
             return _lib.DIST_BYTES
         return _lib.DIST_EXACT_F32 if self.exact_f32_ok(queries, False) else _lib.DIST_F64
 
-    def choose_mode_device(self, q: torch.Tensor, codes: bool) -> int:
+    def choose_mode_device(self, q: torch.Tensor, codes: bool,
+                           stats: tuple[bool, float, float] | None = None) -> int:
         """:meth:`choose_mode` for queries already on this GPU: the same rules, evaluated by a few
-        device reductions and one small copy back, instead of a host pass over the batch."""
+        device reductions and one small copy back, instead of a host pass over the batch.
+        ``stats``: ``(integer, min, max)`` of ``q`` when the caller has read them already."""
         if q.numel() == 0:
             return _lib.DIST_F64
-        # integrality, minimum and maximum in q's own dtype (exact for float32 and float64 alike)
-        lo_q, hi_q = torch.aminmax(q)
-        st = torch.stack([(q != torch.round(q)).any().to(q.dtype), lo_q, hi_q]).to(torch.float64).cpu()
-        integer = not bool(st[0])
+        if stats is None:
+            # integrality, minimum and maximum in q's own dtype (exact for float32 and float64 alike)
+            lo_q, hi_q = torch.aminmax(q)
+            st = torch.stack([(q != torch.round(q)).any().to(q.dtype), lo_q, hi_q]).to(torch.float64).cpu()
+            stats = (not bool(st[0]), float(st[1]), float(st[2]))
+        integer, q_lo, q_hi = stats
         if self.metric == "cosine" or not integer:
             return _lib.DIST_F64
         rows_ok = codes or self.vector_bytes is not None
-        if self.dim % 4 == 0 and rows_ok and float(st[1]) >= 0 and float(st[2]) <= 255:
+        if self.dim % 4 == 0 and rows_ok and q_lo >= 0 and q_hi <= 255:
             return _lib.DIST_BYTES
         if codes:
             lo, hi = np.zeros(self.dim), np.full(self.dim, 255.0)

@@ -29,6 +29,7 @@ import numpy as np
 import torch
 from numpy.typing import ArrayLike, NDArray
 
+from . import _lib
 from .engine import DeviceGraph
 from .validation import (
     NATIVE_ARRAYS,
@@ -297,6 +298,45 @@ class HNSWIndex:
         prepare(rows, self._metric, out=staged.numpy(), checked_finite=True)
         return staged
 
+    def _device_queries(self, queries: torch.Tensor) -> _Uploaded:
+        """Queries already on the GPU, with :meth:`_prepare`'s checks and messages (shape, real
+        dtype, width, NaN/inf, cosine zero rows, float32 overflow) and its values, read back as one
+        small copy that also carries the statistics picking the distance arithmetic."""
+        if queries.ndim != 2:
+            raise ValueError(f"vectors must be a 2-D array, got shape {tuple(queries.shape)}")
+        if queries.dtype == torch.bool or queries.is_complex():
+            dtype = str(queries.dtype).removeprefix("torch.")
+            raise ValueError(f"vectors must contain real numbers, got dtype {dtype}")
+        if queries.shape[1] != self._dim:
+            raise ValueError(f"vectors has dimension {queries.shape[1]}, expected {self._dim}")
+        g = self.device_graph
+        with torch.cuda.device(queries.device):
+            if queries.numel() == 0:
+                return _Uploaded(queries.to(torch.float32).contiguous(), _lib.DIST_F64)
+            raw_finite = torch.isfinite(queries).all()
+            zero_rows = torch.zeros((), dtype=torch.bool, device=queries.device)
+            if self._metric == "cosine":
+                q64 = queries.to(torch.float64)
+                norms = torch.linalg.norm(q64, dim=1, keepdim=True)
+                zero_rows = (norms == 0).any()
+                rows = (q64 / norms).to(torch.float32).contiguous()
+            else:
+                rows = queries.to(torch.float32).contiguous()
+            lo, hi = torch.aminmax(rows)
+            flags = torch.stack([raw_finite.double(), zero_rows.double(),
+                                 torch.isfinite(rows).all().double(),
+                                 (rows != torch.round(rows)).any().double(), lo.double(),
+                                 hi.double()]).cpu().tolist()
+        if not flags[0]:
+            raise ValueError("vectors contains NaN or infinite values")
+        if flags[1]:
+            rows_host = torch.flatnonzero(norms[:, 0] == 0)[:5].cpu().tolist()
+            raise ValueError(f"cosine distance is undefined for zero vectors (rows {rows_host})")
+        if not flags[2]:
+            raise ValueError("vectors overflow float32 (values beyond about 3.4e38)")
+        mode = g.choose_mode_device(rows, False, stats=(not flags[3], flags[4], flags[5]))
+        return _Uploaded(rows, mode)
+
     def _check_search_args(self, k: int, ef: Any) -> tuple[int, Any]:
         if len(self) == 0:
             raise ValueError("cannot search an empty index")
@@ -366,12 +406,7 @@ class HNSWIndex:
         allowed = self._check_filter(filter)
         on_device = isinstance(queries, torch.Tensor) and queries.is_cuda
         if on_device:
-            if queries.ndim != 2 or queries.shape[1] != self._dim:
-                raise ValueError(f"queries must have shape (nq, {self._dim})")
-            prepared: Any = queries.to(torch.float32)
-            if self._metric == "cosine":
-                q64 = queries.to(torch.float64)
-                prepared = (q64 / torch.linalg.norm(q64, dim=1, keepdim=True)).to(torch.float32)
+            prepared: Any = self._device_queries(queries)
         elif allowed is not None and not allowed.any():
             prepared = self._prepare(queries)  # validated; no device work follows
         else:

@@ -198,20 +198,26 @@ void hnsw_b200_close(void *handle);
 int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *args, void *stream);
 
 /* Batched search without any device allocation, for callers that are not allowed to allocate
- * GPU memory: code inside CUDA-graph-captured or real-time serving loops, plugins whose host owns
- * every device allocation, processes under a hard device-memory budget. No counterpart in the
- * reference (its search runs on the CPU). It runs the same unfiltered search kernel as
- * hnsw_b200_search, with all working memory taken from one fixed 32 MiB array inside the library
- * image, which every GPU that loads the library holds until the process exits.
- *   - limits: at most 1,048,576 queries per call; no filter; the graph's per-warp visited bitmap
- *     (n / 8 bytes) must fit several times in the array, which bounds n at about 60 million
- *     nodes; a query that outgrows its share returns HNSW_B200_ERETRY (use hnsw_b200_search);
- *   - the first call on each device looks up the array's device address; make that first call
- *     before any stream capture;
+ * GPU memory: real-time serving loops where an allocation would stall the loop, plugins whose host
+ * owns every device allocation through its own pool, processes under a hard device-memory budget.
+ * No counterpart in the reference (its search runs on the CPU). It runs the same unfiltered search
+ * kernel as hnsw_b200_search, with all working memory taken from one fixed 32 MiB array inside the
+ * library image, which every GPU that loads the library holds until the process exits.
+ *   - limits: at most 1,048,576 queries per call; no filter (allowed must be NULL) and no start
+ *     order (priority must be NULL; allowed_fraction is not read); the graph's per-warp visited
+ *     bitmap (n / 8 bytes) must fit several times in the array, which bounds n at about 60 million
+ *     nodes (larger graphs return HNSW_B200_EINVAL before any GPU work);
+ *   - fewer queries run at once than in hnsw_b200_search: as many warp slots as fit in the array
+ *     (each holds an n / 8-byte bitmap, a list of marked ids, a 4 KB hash and a tie stack), e.g.
+ *     about 228 slots (57 blocks) at 1M nodes against 740 blocks for hnsw_b200_search on a B200;
+ *   - a query that outgrows its share (the upper-layer visited hash) is left unwritten and the
+ *     call returns HNSW_B200_ERETRY; the other queries' outputs are complete (search the failed
+ *     ones with hnsw_b200_search);
+ *   - each call looks up the array's device address on the current device (no cached pointer);
  *   - every call uses the same array and leaves its contents behind (the counters and bitmaps are
  *     cleared at the start of each call): calls that overlap on the GPU -- on two streams, or two
  *     host threads -- race and must not be issued;
- *   - it synchronises `stream` once to read the overflow count. */
+ *   - it waits for `stream` once, to read the overflow count into host memory, before returning. */
 int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph, const hnsw_b200_search_args_t *args,
                              void *stream);
 

@@ -109,15 +109,63 @@ def test_quantized_search_and_fused_rerank_match_reference(name: str, locality: 
         np.testing.assert_array_equal(dists, case[f"dists_r{r}"])
 
 
-def test_single_query_search_matches_batch() -> None:
+@pytest.mark.parametrize("name", ["int_l2", "cont_l2", "cont_ip", "cont_cosine", "mix10k_filtered"])
+def test_single_query_search_matches_reference_fixtures(name: str) -> None:
+    """HNSWIndex.search, one query at a time (the latency path when unfiltered), against the
+    reference's outputs row by row (its search is its batch path on one row, index.py:244-273),
+    with the work counters summed over the rows."""
+    case = load_golden(f"search_{name}")
+    arrays, ep, ml = case_arrays(case, name)
+    metric = str(case["metric"])
+    M = (arrays["links0"].shape[1] - 1) // 2
+    index = _index(arrays, ep, ml, metric, M)
+    k = int(case["k"])
+    rows = range(min(40, case["queries"].shape[0]))
+    for mi, mask, ef in iter_search_runs(case):
+        index.reset_counters()
+        for row in rows:
+            ids, dists = index.search(case["queries"][row], k=k, ef=ef, filter=mask)
+            np.testing.assert_array_equal(ids, case[f"ids_m{mi}_ef{ef}"][row],
+                                          err_msg=f"{name} m{mi} ef{ef} row {row}")
+            np.testing.assert_array_equal(dists, case[f"dists_m{mi}_ef{ef}"][row])
+        if len(rows) == case["queries"].shape[0]:
+            st = index.stats()
+            np.testing.assert_array_equal([st.distance_computations, st.hops],
+                                          case[f"ctr_m{mi}_ef{ef}"])
+
+
+def test_device_queries_are_checked_like_host_queries() -> None:
+    """CUDA-tensor queries get the host validator's checks and messages (_validation.py:28-40,
+    metrics.py:42-68): NaN/inf, width, dtype, cosine zero rows."""
+    import torch
+
     case = load_golden("search_cont_l2")
     arrays, ep, ml = case_arrays(case, "cont_l2")
     index = _index(arrays, ep, ml, "l2", 8)
-    ids, dists = index.batch_search(case["queries"][:12], k=5, ef=30)
-    for row in range(12):
-        a, b = index.search(case["queries"][row], k=5, ef=30)
-        np.testing.assert_array_equal(a, ids[row])
-        np.testing.assert_array_equal(b, dists[row])
+    q = np.ascontiguousarray(case["queries"], dtype=np.float32)
+    want = index.batch_search(q, k=10, ef=30)
+    for dtype in (torch.float32, torch.float64):
+        got = index.batch_search(torch.from_numpy(q).to("cuda", dtype), k=10, ef=30)
+        for a, b in zip(want, got, strict=True):
+            np.testing.assert_array_equal(a, b.cpu().numpy())
+        for bad_value in (np.nan, np.inf, -np.inf):
+            bad = torch.from_numpy(q).to("cuda", dtype)
+            bad[3, 1] = bad_value
+            with pytest.raises(ValueError, match="vectors contains NaN or infinite values"):
+                index.batch_search(bad, k=10, ef=30)
+    with pytest.raises(ValueError, match="expected 10"):
+        index.batch_search(torch.zeros((2, 9), device="cuda"), k=10, ef=30)
+    with pytest.raises(ValueError, match="2-D"):
+        index.batch_search(torch.zeros(10, device="cuda"), k=10, ef=30)
+    with pytest.raises(ValueError, match="real numbers"):
+        index.batch_search(torch.zeros((2, 10), dtype=torch.bool, device="cuda"), k=10, ef=30)
+    cos = load_golden("search_cont_cosine")
+    arrays, ep, ml = case_arrays(cos, "cont_cosine")
+    cindex = _index(arrays, ep, ml, "cosine", (arrays["links0"].shape[1] - 1) // 2)
+    zero = torch.from_numpy(np.ascontiguousarray(cos["queries"][:4], dtype=np.float32)).cuda()
+    zero[2] = 0.0
+    with pytest.raises(ValueError, match=r"zero vectors \(rows \[2\]\)"):
+        cindex.batch_search(zero, k=10, ef=30)
 
 
 def test_host_query_forms_agree_and_reject_nan_alike() -> None:
