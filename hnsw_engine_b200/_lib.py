@@ -98,6 +98,7 @@ class ExactArgs(ctypes.Structure):
         ("out_filter_max_error", ctypes.c_void_p),
         ("out_candidates", ctypes.c_void_p),
         ("out_launches", ctypes.c_void_p),
+        ("out_filter_error_bound", ctypes.c_void_p),
     ]
 
 

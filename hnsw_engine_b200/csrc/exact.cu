@@ -565,7 +565,8 @@ template <typename T>
 __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq, int32_t k,
                             int32_t metric, const double *xnorm, const double *qnorm,
                             const float *cand_val, const int32_t *cand_id, const int32_t *cand_cnt,
-                            int32_t cap, const float *thr, int64_t *out_ids, double *out_d) {
+                            int32_t cap, const float *thr, int64_t *out_ids, double *out_d,
+                            unsigned long long *err_max) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warps = blockDim.x >> 5;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -579,9 +580,11 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
     const T *qv = queries + int64_t(q) * dim;
     const double qn = qnorm[q];
     int a = 0;
+    double err = 0.0;  // largest |filter value - exact distance| over this lane's survivors
     for (int base = 0; base < m; base += 32) {
         const int i = base + lane;
-        bool has = i < m && cand_val[int64_t(q) * cap + i] <= t;
+        const float approx = i < m ? cand_val[int64_t(q) * cap + i] : INFINITY;
+        bool has = i < m && approx <= t;
         int32_t id = has ? cand_id[int64_t(q) * cap + i] : -1;
         double d = INFINITY;
         if (has) {
@@ -602,6 +605,7 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
                     acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[j]), xn), __ddiv_rn(double(qv[j]), qn)));
                 d = __dsub_rn(1.0, acc);
             }
+            err = fmax(err, fabs(double(approx) - d));
         }
         uint32_t am = __ballot_sync(0xffffffffu, has);
         while (am) {
@@ -640,6 +644,12 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
         out_ids[int64_t(q) * k + r] = r < a ? int64_t(Ai[r]) : -1;
         out_d[int64_t(q) * k + r] = r < a ? Ad[r] : INFINITY;
     }
+    // Non-negative doubles order as their bit patterns: an integer maximum over the warp, then
+    // one atomic per query.
+    unsigned long long eb = static_cast<unsigned long long>(__double_as_longlong(err));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) eb = max(eb, __shfl_xor_sync(0xffffffffu, eb, o));
+    if (lane == 0 && eb) atomicMax(err_max, eb);
 }
 
 // Error bound of the filter arithmetic and the per-query margins (2 e_q).
@@ -727,16 +737,21 @@ struct Scratch {
 
 size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Candidate lists take about CAND_BYTES of scratch: (queries per chunk) x cap x 8 bytes.
+constexpr int64_t CAND_BYTES = int64_t(4) << 30;
+
+// One attempt at the whole batch with candidate lists of at least cap_min entries. Returns
+// HNSW_B200_ERETRY with *cap_needed set when a query's candidates outgrew its list (many rows
+// within the margin of the k-th distance, e.g. exact ties); the caller retries with that size.
 template <typename T>
-int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
+int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap_min,
+                    int64_t *cap_needed) {
     const int64_t n = a->n, nq_all = a->nq;
     const int dim = a->dim, k = a->k, metric = a->metric;
     const int terms = a->integer_valued && metric != HNSW_B200_COSINE ? 1 : 3;
     const int seg = (dim + BK - 1) / BK * BK;
     const int kp = seg * terms;
     const int64_t n_pad = (n + BN - 1) / BN * BN;
-    const int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
-    const int64_t q_pad = (QB + BM - 1) / BM * BM;
     int sms = 148;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -744,9 +759,16 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
 
     // Candidate capacity: pass one keeps every row of its prefix; pass two about k * n / prefix.
     const int64_t prefix = std::min<int64_t>(n, std::max<int64_t>(int64_t(64) * k, 32768));
+    const int64_t qb_max = std::min<int64_t>(nq_all, 8192);
     int64_t cap = std::max<int64_t>(
         prefix, std::min<int64_t>(n, 24 * int64_t(k) * (n / std::max<int64_t>(prefix, 1)) + 4096));
-    cap = std::min<int64_t>(cap, std::max<int64_t>(prefix, (int64_t(4) << 30) / (8 * QB)));
+    cap = std::min<int64_t>(cap, std::max<int64_t>(prefix, CAND_BYTES / (8 * qb_max)));
+    cap = std::max<int64_t>(cap, std::min<int64_t>(cap_min, n));
+    // Queries per chunk: up to 8192, fewer when a retry needs longer candidate lists.
+    int64_t QB = qb_max;
+    if (QB * cap * 8 > CAND_BYTES)
+        QB = std::min<int64_t>(qb_max, std::max<int64_t>(BM, CAND_BYTES / (8 * cap) / BM * BM));
+    const int64_t q_pad = (QB + BM - 1) / BM * BM;
 
     static thread_local Scratch buf;
     size_t off = 0;
@@ -769,6 +791,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
     const size_t o_ci = carve(size_t(QB) * cap * 4);
     const size_t o_err = carve(16);
     const size_t o_mx = carve(16);
+    const size_t o_fe = carve(16);
     if (int rc = buf.get(off)) return rc;
     char *B = static_cast<char *>(buf.p);
     auto *xb = reinterpret_cast<__nv_bfloat16 *>(B + o_xb);
@@ -814,6 +837,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
     if (rsm > 200 * 1024) return fail(HNSW_B200_EINVAL, "k too large for the rerank kernel");
     XT(cudaFuncSetAttribute(rerank_topk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(rsm)));
     XT(cudaMemsetAsync(err, 0, 16, s));
+    auto *ferr = reinterpret_cast<unsigned long long *>(B + o_fe);  // measured filter error (bits)
+    XT(cudaMemsetAsync(ferr, 0, 8, s));
     std::vector<float> inf(static_cast<size_t>(QB), INFINITY);
     std::vector<int32_t> hc(static_cast<size_t>(QB));
     double max_margin = 0.0;
@@ -873,24 +898,34 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s) {
             worst = std::max(worst, hc[size_t(i)]);
             total_cand += hc[size_t(i)];
         }
-        if (worst > cap)
+        if (worst > cap) {
+            *cap_needed = worst;
             return fail(HNSW_B200_ERETRY, "exact knn: candidate buffer overflow (" + std::to_string(worst) +
                                               " > " + std::to_string(cap) + ")");
+        }
         // The k-th smallest candidate is the global k-th approximate distance: final threshold.
         select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nq), k, mg, th, tau);
         rerank_topk<T><<<int((nq + wpb - 1) / wpb), wpb * 32, rsm, s>>>(
             X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), th,
-            a->out_ids + q0 * k, a->out_dists + q0 * k);
+            a->out_ids + q0 * k, a->out_dists + q0 * k, ferr);
         XT(cudaGetLastError());
         launches += 3;
-        if (a->out_filter_max_error) {
+        if (a->out_filter_error_bound) {
             std::vector<float> hm(static_cast<size_t>(nq));
             XT(cudaMemcpyAsync(hm.data(), mg, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
             XT(cudaStreamSynchronize(s));
             for (float v : hm) max_margin = std::max(max_margin, double(v));
         }
     }
-    if (a->out_filter_max_error) *a->out_filter_max_error = max_margin / 2.0;
+    if (a->out_filter_error_bound) *a->out_filter_error_bound = max_margin / 2.0;
+    if (a->out_filter_max_error) {
+        unsigned long long bits = 0;
+        XT(cudaMemcpyAsync(&bits, ferr, 8, cudaMemcpyDeviceToHost, s));
+        XT(cudaStreamSynchronize(s));
+        double e = 0.0;
+        std::memcpy(&e, &bits, 8);
+        *a->out_filter_max_error = e;
+    }
     if (a->out_candidates) *a->out_candidates = total_cand;
     if (a->out_launches) *a->out_launches = launches;
     return 0;
@@ -906,10 +941,18 @@ extern "C" int hnsw_b200_exact_knn(const hnsw_b200_exact_args_t *a, void *stream
         return fail(HNSW_B200_EINVAL, "need n >= 1, dim >= 1, 1 <= k <= n");
     if (a->metric < 0 || a->metric > 2) return fail(HNSW_B200_EINVAL, "unknown metric");
     if (a->nq == 0) return 0;
+    if (a->dtype != HNSW_B200_F32 && a->dtype != HNSW_B200_U8)
+        return fail(HNSW_B200_EINVAL, "unsupported dtype");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    switch (a->dtype) {
-        case HNSW_B200_F32: return exact_knn_typed<float>(a, s);
-        case HNSW_B200_U8: return exact_knn_typed<uint8_t>(a, s);
-        default: return fail(HNSW_B200_EINVAL, "unsupported dtype");
+    // A candidate overflow re-runs the batch with lists long enough for the largest count seen
+    // (plus a quarter); a list of n entries can never overflow, so this ends.
+    int64_t cap_min = 0;
+    for (int attempt = 0; attempt < 4; attempt++) {
+        int64_t need = 0;
+        const int rc = a->dtype == HNSW_B200_F32 ? exact_knn_typed<float>(a, s, cap_min, &need)
+                                                 : exact_knn_typed<uint8_t>(a, s, cap_min, &need);
+        if (rc != HNSW_B200_ERETRY || need <= 0) return rc;
+        cap_min = std::max(cap_min, need + need / 4 + 64);
     }
+    return fail(HNSW_B200_ERETRY, "exact knn: candidate lists still overflowed after retries");
 }

@@ -23,9 +23,10 @@ from .validation import as_matrix, check_k, validate_metric
 
 @dataclass
 class ExactStats:
-    filter_max_error: float
+    filter_max_error: float    # measured: largest |filter value - float64 distance| re-scored
     candidates: int
     launches: int
+    filter_error_bound: float  # derived bound of the filter's error (margins are twice it)
 
 
 def _integer_small(a: Any) -> bool:
@@ -86,6 +87,7 @@ def exact_search(
     ids = torch.empty((nq, k), dtype=torch.int64, device=dev)
     dists = torch.empty((nq, k), dtype=torch.float64, device=dev)
     err = ctypes.c_double(0.0)
+    bound = ctypes.c_double(0.0)
     cand = ctypes.c_int64(0)
     launches = ctypes.c_int64(0)
     args = _lib.ExactArgs(
@@ -93,12 +95,12 @@ def exact_search(
         dtype=_lib_dtype(x), dim=dim, n=n, nq=nq, k=k, metric=_lib.METRIC_CODES[metric],
         integer_valued=int(integer), reserved=0, out_ids=ids.data_ptr(), out_dists=dists.data_ptr(),
         out_filter_max_error=ctypes.addressof(err), out_candidates=ctypes.addressof(cand),
-        out_launches=ctypes.addressof(launches),
+        out_launches=ctypes.addressof(launches), out_filter_error_bound=ctypes.addressof(bound),
     )
     with torch.cuda.device(dev):
         stream = torch.cuda.current_stream(dev).cuda_stream
         _lib.check(lib.hnsw_b200_exact_knn(ctypes.byref(args), ctypes.c_void_p(stream)))
-    stats = ExactStats(err.value, cand.value, launches.value)
+    stats = ExactStats(err.value, cand.value, launches.value, bound.value)
     out: Any = (ids, dists) if on_device else (ids.cpu().numpy(), dists.cpu().numpy())
     return (*out, stats) if return_stats else out
 

@@ -140,6 +140,7 @@ def exact(k: int = 100) -> None:
         flops = 2.0 * queries.shape[0] * data.shape[0] * data.shape[1]
         _emit(config="exact", data=label, nq=queries.shape[0], k=k, seconds=s, qps=queries.shape[0] / s,
               gemm_tflops=flops / s / 1e12, filter_max_error=st.filter_max_error,
+              filter_error_bound=st.filter_error_bound,
               candidates_per_query=st.candidates / queries.shape[0])
     img = synthetic.image_like(60000, seed=synthetic.IMAGE_DATA_SEED)
     iq = synthetic.image_like(10000, seed=synthetic.IMAGE_QUERY_SEED)
@@ -153,6 +154,7 @@ def exact(k: int = 100) -> None:
     flops = 2.0 * 10000 * 60000 * 784
     _emit(config="exact", data="image-like 60K x 784 uint8", nq=10000, k=k, seconds=s, qps=10000 / s,
           gemm_tflops=flops / s / 1e12, filter_max_error=st.filter_max_error,
+              filter_error_bound=st.filter_error_bound,
           candidates_per_query=st.candidates / 10000)
 
 

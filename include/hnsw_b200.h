@@ -154,15 +154,20 @@ typedef struct hnsw_b200_exact_args {
     int32_t reserved;
     int64_t *out_ids;              /* (nq, k) int64, ascending (distance, id) */
     double *out_dists;             /* (nq, k) float64 exact distances */
-    double *out_filter_max_error;  /* host: largest error bound of the BF16/FP32 filter, or NULL */
+    double *out_filter_max_error;  /* host: largest |filter value - float64 distance| measured over
+                                      every re-scored candidate of the call, or NULL */
     int64_t *out_candidates;       /* host: candidates re-scored in float64, or NULL */
     int64_t *out_launches;         /* host: kernel launches made, or NULL */
+    double *out_filter_error_bound; /* host: largest derived bound e_q of the filter's error (the
+                                      margin is 2 e_q), or NULL; the measured error never exceeds it */
 } hnsw_b200_exact_args_t;
 
 /* Exact k nearest neighbours by brute force on the tensor cores (BF16 filter with FP32
  * accumulation and a derived error margin, then float64 re-rank of the survivors, ties to the
  * lower id). Replaces oracle.exact_search (src/hnsw_engine/oracle.py:35-126). Synchronises
- * `stream`. */
+ * `stream`. When more rows fall within a query's margin than its candidate list holds (many exact
+ * ties at the k-th distance), the call re-runs with longer lists (fewer queries per chunk) instead
+ * of failing. */
 int hnsw_b200_exact_knn(const hnsw_b200_exact_args_t *args, void *stream);
 
 /* ---- Early-termination network (no reference counterpart): 12 -> 64 -> 64 -> 1, ReLU.

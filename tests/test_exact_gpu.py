@@ -96,3 +96,63 @@ def test_mixture_1m_shape_subset_matches_oracle() -> None:
     o_ids, o_d = exact.exact_search(data, queries, 100, "l2")
     np.testing.assert_array_equal(ids, o_ids)
     np.testing.assert_array_equal(dists, o_d)
+
+
+def _sample_rows(nq: int, count: int) -> np.ndarray:
+    """Query rows spread over the whole batch (both 8192-query chunks of a 10K batch)."""
+    return np.unique(np.linspace(0, nq - 1, count).round().astype(np.int64))
+
+
+def test_full_mixture_config_1m_x_128_k100_matches_oracle() -> None:
+    """The 1M x 128 mixture with its 10K queries at k = 100, searched in full on the GPU; a spread
+    sample of 256 queries against the CPU restatement of oracle.exact_search over all 1M rows.
+    Integer data at d = 128: the filter arithmetic is exact, so the measured error is 0."""
+    from hnsw_engine_b200 import synthetic
+    from hnsw_engine_b200.exact_knn import exact_search
+    from oracle import exact
+
+    data = synthetic.mixture(1_000_000, seed=synthetic.DATA_SEED)
+    queries = synthetic.mixture(10_000, seed=synthetic.QUERY_SEED)
+    ids, dists, st = exact_search(data, queries, 100, "l2", return_stats=True)
+    rows = _sample_rows(10_000, 256)
+    o_ids, o_d = exact.exact_search(data, queries[rows], 100, "l2")
+    np.testing.assert_array_equal(ids[rows], o_ids)
+    np.testing.assert_array_equal(dists[rows], o_d)
+    assert st.filter_max_error == 0.0
+    assert st.filter_max_error <= st.filter_error_bound
+
+
+def test_full_image_config_60k_x_784_k100_matches_oracle() -> None:
+    """The 60K x 784 image-like uint8 set with its 10K queries at k = 100 on the GPU; a spread
+    sample of 256 queries against the CPU oracle, ids and distances bit-exact. Sums reach beyond
+    2^24 here, so the filter is approximate: its measured error must stay within the bound."""
+    from hnsw_engine_b200 import synthetic
+    from hnsw_engine_b200.exact_knn import exact_search
+    from oracle import exact
+
+    data = synthetic.image_like(60_000, seed=synthetic.IMAGE_DATA_SEED).astype(np.uint8)
+    queries = synthetic.image_like(10_000, seed=synthetic.IMAGE_QUERY_SEED).astype(np.uint8)
+    ids, dists, st = exact_search(data, queries, 100, "l2", return_stats=True)
+    rows = _sample_rows(10_000, 256)
+    o_ids, o_d = exact.exact_search(data, queries[rows], 100, "l2")
+    np.testing.assert_array_equal(ids[rows], o_ids)
+    np.testing.assert_array_equal(dists[rows], o_d)
+    assert 0.0 <= st.filter_max_error <= st.filter_error_bound
+
+
+def test_candidate_overflow_is_retried_with_longer_lists() -> None:
+    """50,000 identical rows all tie at every query's k-th distance: far more rows fall within the
+    margin than the first candidate lists hold. The call re-runs with longer lists and returns the
+    exact answer (ties to the lower id) instead of failing."""
+    from hnsw_engine_b200.exact_knn import exact_search
+    from oracle import exact
+
+    rng = np.random.default_rng(11)
+    data = rng.integers(0, 256, (100_000, 32)).astype(np.float32)
+    data[10_000:60_000] = 7.0  # one row repeated 50,000 times
+    queries = np.full((40, 32), 7.0, np.float32) + rng.integers(0, 2, (40, 32)).astype(np.float32)
+    ids, dists, st = exact_search(data, queries, 10, "l2", return_stats=True)
+    o_ids, o_d = exact.exact_search(data, queries, 10, "l2")
+    np.testing.assert_array_equal(ids, o_ids)
+    np.testing.assert_array_equal(dists, o_d)
+    assert st.candidates >= 40 * 50_000
