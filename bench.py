@@ -55,6 +55,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--k", type=int, default=10)
     p.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the other configurations (quantized, filtered, planner, exact k-NN)")
     return p.parse_args()
 
 
@@ -217,6 +219,7 @@ def run_reference(args: argparse.Namespace) -> None:
             values.append(res["value"])
     value = statistics.median(values)
     res["value"] = value
+    res["cpu_model"] = cpu_model()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * len(queries) / value,
@@ -244,6 +247,99 @@ def timed_steps(step, steps: int, stream) -> list[float]:
         ends[i].record(stream)
     torch.cuda.synchronize()
     return [a.elapsed_time(b) for a, b in zip(starts, ends, strict=True)]
+
+
+def other_configs(index, workload: str, queries: np.ndarray, q_dev, gt_ids, gt_d, k: int, ef: int,
+                  stream) -> dict:
+    """The workload's other configurations on the same graph and queries, device-resident and timed
+    with CUDA events (median of 3 launches; 1 for the slowest): int8 scalar-quantizer codes with the
+    fused exact re-rank of the beam at the operating efSearch; Bernoulli and prefix filters at
+    p = 0.5 / 0.1 / 0.01 at the same efSearch (recall against the exact neighbours among the
+    allowed rows) and the selectivity planner at p = 0.01; the tensor-core exact k-NN at k = 100."""
+    import torch
+
+    from hnsw_engine_b200 import synthetic
+    from hnsw_engine_b200.engine import pack_mask, to_device
+    from hnsw_engine_b200.exact_knn import exact_search
+    from hnsw_engine_b200.quantization import QuantizedIndex
+
+    g = index.device_graph
+    dev = q_dev.device
+    nq = queries.shape[0]
+    metric = index.metric
+    out: dict = {}
+
+    def med(fn, reps: int = 3) -> float:
+        fn()
+        torch.cuda.synchronize()
+        return float(np.median(timed_steps(fn, reps, stream)))
+
+    qi = QuantizedIndex(index)
+    code_q = torch.from_numpy(qi.quantizer.transform_queries(queries, metric)).to(dev)
+    held: dict = {}
+
+    def run_codes():
+        held["r"] = qi.batch_search_device(code_q, q_dev, k, ef, ef)
+
+    ms = med(run_codes)
+    ids, d = held["r"]
+    out["int8_codes_fused_rerank"] = {
+        "ef": ef, "rerank": ef, "step": float(qi.quantizer.step), "ms": ms, "qps": nq / ms * 1e3,
+        "recall_at_10": recall_of(ids.cpu().numpy(), d.cpu().numpy(), gt_ids, gt_d, k)}
+
+    n = g.n
+    for kind in ("bernoulli", "prefix"):
+        for p in (0.5, 0.1, 0.01):
+            mask = synthetic.bernoulli_mask(n, p) if kind == "bernoulli" else synthetic.prefix_mask(n, p)
+            sub = torch.from_numpy(np.flatnonzero(mask)).to(dev)
+            t_ids, t_d = exact_search(g.vectors[sub].contiguous(), q_dev, k, metric)
+            t_ids, t_d = sub[t_ids].cpu().numpy(), t_d.cpu().numpy()
+            bitmap = to_device(pack_mask(g.internal_mask(mask)).view(np.int32), torch.int32, dev)
+            frac = float(mask.mean())
+
+            def run_filtered():
+                held["r"] = g.search(q_dev, k, ef, allowed=bitmap, allowed_fraction=frac,
+                                     counters=False)
+
+            ms = med(run_filtered, reps=1 if p < 0.05 else 3)
+            ids, d, _ = held["r"]
+            entry = {"ef": ef, "ms": ms, "qps": nq / ms * 1e3,
+                     "recall_at_10": recall_of(ids.cpu().numpy(), d.cpu().numpy(), t_ids, t_d, k)}
+            if p < 0.05:
+                def run_planner():
+                    held["r"] = index.batch_search(q_dev, k=k, ef=ef, filter=mask, exact_below=0.05)
+
+                ms = med(run_planner)
+                ids, d = held["r"]
+                entry["planner_exact_below_0.05"] = {
+                    "ms": ms, "qps": nq / ms * 1e3,
+                    "recall_at_10": recall_of(ids.cpu().numpy(), d.cpu().numpy(), t_ids, t_d, k)}
+            out[f"filtered_{kind}_p{p}"] = entry
+
+    kx = 100
+    exact_search(g.vectors, q_dev, kx)  # scratch allocated outside the timing
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, _, st = exact_search(g.vectors, q_dev, kx, metric, return_stats=True)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    flops = 2.0 * nq * n * g.dim
+    out["exact_knn_k100"] = {
+        "seconds": sec, "qps": nq / sec, "tflops": flops / sec / 1e12,
+        "filter_max_error_measured": st.filter_max_error,
+        "filter_error_bound": st.filter_error_bound,
+        "candidates_per_query": st.candidates / nq, "launches": st.launches}
+    return out
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def main() -> None:
@@ -285,42 +381,52 @@ def main() -> None:
     mode = g.choose_mode(queries, False)
     row_bytes = dim * (1 if mode == 2 else 4)
 
-    # Exact ground truth; plain fixed-ef operating point: smallest efSearch reaching the target.
+    # Held-out protocol: every operating point is fixed on the validation queries (seed 9), then
+    # both arms are timed and scored on the benchmark queries (seed 1), which nothing was tuned on.
+    from hnsw_engine_b200.train_stop import VALIDATION_SEED
+
+    val_q = prepare(graphs.workload_queries(args.workload, nq=nq, seed=VALIDATION_SEED), metric)
+    val_dev = torch.from_numpy(val_q).to(dev)
     gt_ids, gt_d = ground_truth(g.vectors, queries, k, metric)
+    vgt_ids, vgt_d = ground_truth(g.vectors, val_q, k, metric)
+
+    def val_recall(ef: int) -> float:
+        ids, dists, _ = g.search(val_dev, k, ef, dist_mode=mode)
+        return recall_of(ids.cpu().numpy(), dists.cpu().numpy(), vgt_ids, vgt_d, k)
+
+    # Plain fixed-ef operating point: the smallest efSearch on the ladder reaching the target on
+    # the validation queries, then the smallest integer efSearch between the rung below and it.
     sweep = {}
     ef_op = EF_LADDER[-1]
     for ef in EF_LADDER:
-        ids, dists, _ = g.search(q_dev, k, ef, dist_mode=mode)
-        sweep[ef] = recall_of(ids.cpu().numpy(), dists.cpu().numpy(), gt_ids, gt_d, k)
+        sweep[ef] = val_recall(ef)
         if sweep[ef] >= RECALL_TARGET:
             ef_op = ef
             break
-    # The same operating point without the ladder's granularity: the smallest integer efSearch
-    # between the last rung below the target and ef_op (recall rises with ef on these graphs).
     i_op = EF_LADDER.index(ef_op)
     lo, hi = (EF_LADDER[i_op - 1] if i_op else k - 1), ef_op
-    ef_fine, rec_fine = ef_op, sweep[ef_op]
+    ef_fine = ef_op
     while hi - lo > 1:
         mid = (lo + hi) // 2
-        ids, dists, _ = g.search(q_dev, k, mid, dist_mode=mode)
-        r = recall_of(ids.cpu().numpy(), dists.cpu().numpy(), gt_ids, gt_d, k)
-        if r >= RECALL_TARGET:
-            hi, ef_fine, rec_fine = mid, mid, r
+        if val_recall(mid) >= RECALL_TARGET:
+            hi = ef_fine = mid
         else:
             lo = mid
     if rank == 0:
         try:
             (ROOT / "graphs" / args.workload / "operating_point.json").write_text(
-                json.dumps({"ef": ef_op, "recall": sweep[ef_op]}))
+                json.dumps({"ef": ef_op, "validation_recall": sweep[ef_op]}))
         except OSError:
             pass
 
-    # Learned stop: the trained network (trained now if none is stored), its threshold tuned on
-    # the same queries for the same recall target (equal measured recall).
+    # Learned stop: the trained network, its threshold tuned on the validation queries for the
+    # recall target. The in-sample threshold (tuned on the benchmark queries themselves) is kept
+    # only as a side figure.
     net = load_or_train(args.workload, device=str(dev))
     cap = net.ef_cap
-    val_threshold = net.threshold
-    thr, _ = tune_threshold(g, net, q_dev, gt_d, k, cap, RECALL_TARGET)
+    thr, val_rec_l = tune_threshold(g, net, val_dev, vgt_d, k, cap, RECALL_TARGET)
+    thr_in, _ = tune_threshold(g, net, q_dev, gt_d, k, cap, RECALL_TARGET)
+    net.threshold = thr
     packed = net.packed()
 
     ids_o = torch.empty((nq, k), dtype=torch.int64, device=dev)
@@ -329,20 +435,32 @@ def main() -> None:
     ids_p = torch.empty_like(ids_o)
     d_p = torch.empty_like(d_o)
     c_p = torch.empty_like(c_o)
+    ids_f = torch.empty_like(ids_o)
+    d_f = torch.empty_like(d_o)
+    c_f = torch.empty_like(c_o)
+    ids_i = torch.empty_like(ids_o)
+    d_i = torch.empty_like(d_o)
+    c_i = torch.empty_like(c_o)
 
     def step_learned():
         g.search(q_dev, k, cap, out=(ids_o, d_o, c_o), dist_mode=mode,
                  stop=(packed, thr, net.slope, net.slope_from))
 
+    def step_in_sample():
+        g.search(q_dev, k, cap, out=(ids_i, d_i, c_i), dist_mode=mode,
+                 stop=(packed, thr_in, net.slope, net.slope_from))
+
     def step_plain():
         g.search(q_dev, k, ef_op, out=(ids_p, d_p, c_p), dist_mode=mode)
 
     def step_fine():
-        g.search(q_dev, k, ef_fine, out=(ids_p, d_p, c_p), dist_mode=mode)
+        g.search(q_dev, k, ef_fine, out=(ids_f, d_f, c_f), dist_mode=mode)
 
     for _ in range(max(3, args.warmup)):
         step_learned()
         step_plain()
+        step_fine()
+        step_in_sample()
     torch.cuda.synchronize()
     launches_per_step = g.last_launches
     alg_bytes = algorithmic_bytes(c_o.cpu().numpy(), arrays, dim, k, row_bytes)
@@ -356,20 +474,24 @@ def main() -> None:
         ms_learned = timed_steps(step_learned, args.steps, stream)
         ms_fine = timed_steps(step_fine, args.steps, stream)
         ms_plain = timed_steps(step_plain, args.steps, stream)
+        ms_in = timed_steps(step_in_sample, max(3, args.steps // 4), stream)
     total_l = max_over_ranks(pg, float(sum(ms_learned)), dev)
     total_p = max_over_ranks(pg, float(sum(ms_plain)), dev)
     fine_qps = job_throughput(world, nq, args.steps, max_over_ranks(pg, float(sum(ms_fine)), dev))
+    in_qps = job_throughput(world, nq, len(ms_in), max_over_ranks(pg, float(sum(ms_in)), dev))
     value = job_throughput(world, nq, args.steps, total_l)
     plain_qps = job_throughput(world, nq, args.steps, total_p)
     mean_ms = total_l / args.steps
     rec_l = recall_of(ids_o.cpu().numpy(), d_o.cpu().numpy(), gt_ids, gt_d, k)
     rec_p = recall_of(ids_p.cpu().numpy(), d_p.cpu().numpy(), gt_ids, gt_d, k)
+    rec_f = recall_of(ids_f.cpu().numpy(), d_f.cpu().numpy(), gt_ids, gt_d, k)
+    rec_i = recall_of(ids_i.cpu().numpy(), d_i.cpu().numpy(), gt_ids, gt_d, k)
     hops_l = float(c_o[:, 1].float().mean())
     hops_p = float(c_p[:, 1].float().mean())
+    hops_f = float(c_f[:, 1].float().mean())
 
     # End to end through the public API with host buffers (numpy in, numpy out): each step copies
     # the float32 queries to the GPU and the ids and distances back. Mean over the steps.
-    net.threshold = thr
     for _ in range(3):  # results held as in the timed loop, so its page-locked buffers exist
         e_ids, e_d = index.batch_search(raw_q, k=k, ef=cap, stop=net)
     torch.cuda.synchronize()
@@ -382,19 +504,13 @@ def main() -> None:
     e2e_value = job_throughput(world, nq, 1, e2e_ms)
     assert np.array_equal(e_ids, ids_o.cpu().numpy()), "e2e results differ from device results"
 
-    # Held out: the threshold tuned on the validation queries (not these), its recall here, and
-    # how often the per-batch audit (2% of each batch against the exact k-NN) falls back to plain
-    # fixed ef, over ten batches of a tenth of the queries.
-    ho_ids, ho_d, ho_c = stopped_search(g, q_dev, k, cap, packed, val_threshold, net.slope,
-                                        net.slope_from)
-    ho_rec = recall_of(ho_ids.cpu().numpy(), ho_d.cpu().numpy(), gt_ids, gt_d, k)
-    net.threshold = val_threshold
+    # The per-batch audit (2% of each batch against the exact k-NN; plain fixed ef on a miss),
+    # over ten batches of a tenth of the queries.
     audits = []
     for part_i, part in enumerate(np.array_split(np.arange(nq), 10)):
         _, _, fell, arec = audited_search(g, q_dev[torch.from_numpy(part).to(dev)], k, cap, net,
                                           ef_op, RECALL_TARGET, seed=part_i)
         audits.append((bool(fell), float(arec)))
-    net.threshold = thr
 
     # Per-query efSearch uniform on 32..512 (the batched-at-scale configuration).
     pq = synthetic.per_query_ef(nq, seed=11, low=32, high=512)
@@ -405,6 +521,8 @@ def main() -> None:
     pq_rec = recall_of(pq_ids.cpu().numpy(), pq_d.cpu().numpy(), gt_ids, gt_d, k)
     pq_bytes = algorithmic_bytes(pq_c.cpu().numpy(), arrays, dim, k, row_bytes)
     pq_mean = max_over_ranks(pg, float(np.median(pq_ms)), dev)
+    more = other_configs(index, args.workload, queries, q_dev, gt_ids, gt_d, k, ef_op, stream) \
+        if world == 1 and not args.no_configs else None
 
     pk = peaks()
     achieved = alg_bytes / (mean_ms / 1000.0) / 1e9
@@ -414,6 +532,10 @@ def main() -> None:
 
         cpu_base = cpu_sample(arrays, ep, ml, queries, k, ef_op, metric, args.cpu_sample_seconds,
                               cpu.default_threads())
+        one = cpu_sample(arrays, ep, ml, queries, k, ef_op, metric, 5.0, 1)
+        cpu_base["single_thread"] = {"value": one["value"], "sample": one["sample"]}
+        cpu_base["cpu_model"] = cpu_model()
+        cpu_base["host_threads"] = os.cpu_count()
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -434,25 +556,28 @@ def main() -> None:
                             f"M={params['M']}, efC={params['ef_construction']}, nq={nq}, k={k}",
                 "method": "learned stop (value) vs plain fixed-ef, equal recall target "
                           f"{RECALL_TARGET}",
+                "protocol": "held out: plain efSearch and the stop threshold fixed on "
+                            f"{nq} validation queries (seed {VALIDATION_SEED}); both arms timed "
+                            "and scored on the benchmark queries (seed 1)",
                 "learned_stop": {"ef_cap": cap, "threshold": thr, "recall_at_10": rec_l,
+                                 "validation_recall_at_10": val_rec_l,
                                  "threshold_slope": net.slope, "slope_from_hops": net.slope_from,
                                  "qps": value, "mean_hops": hops_l,
-                                 "validation_threshold": val_threshold,
-                                 "held_out": {
-                                     "threshold": val_threshold,
-                                     "recall_at_10": ho_rec,
-                                     "mean_hops": float(ho_c[:, 1].float().mean()),
-                                     "audit_batches": len(audits),
-                                     "audit_fallbacks": sum(f for f, _ in audits),
-                                     "audit_sample_recalls": [r for _, r in audits],
-                                 }},
+                                 "audit_batches": len(audits),
+                                 "audit_fallbacks": sum(f for f, _ in audits),
+                                 "audit_sample_recalls": [r for _, r in audits],
+                                 "in_sample": {"threshold": thr_in, "recall_at_10": rec_i,
+                                               "qps": in_qps,
+                                               "note": "threshold tuned on the benchmark queries "
+                                                       "themselves; not the value"}},
                 "plain_fixed_ef": {"ef": ef_op, "recall_at_10": rec_p, "qps": plain_qps,
                                    "mean_hops": hops_p,
                                    "achieved_gbs": alg_bytes_plain / (total_p / args.steps / 1000.0) / 1e9},
                 "learned_over_plain": value / plain_qps,
-                "plain_fixed_ef_fine": {"ef": ef_fine, "recall_at_10": rec_fine, "qps": fine_qps},
+                "plain_fixed_ef_fine": {"ef": ef_fine, "recall_at_10": rec_f, "qps": fine_qps,
+                                        "mean_hops": hops_f},
                 "learned_over_plain_fine": value / fine_qps,
-                "ef_sweep": {str(e): r for e, r in sweep.items()},
+                "validation_ef_sweep": {str(e): r for e, r in sweep.items()},
                 "l2_policy": "inputs larger than L2 (vectors %d MB + links %d MB > 126 MB)"
                              % (arrays["vectors"].nbytes >> 20, np.asarray(arrays["links0"]).nbytes >> 20),
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -461,6 +586,7 @@ def main() -> None:
                                 else "row order"),
                 "per_query_ef_32_512": {"qps": job_throughput(world, nq, 1, pq_mean), "recall_at_10": pq_rec,
                                         "achieved_gbs": pq_bytes / (pq_mean / 1000.0) / 1e9},
+                "configs": more,
             },
             "roofline": {
                 "bound": "hbm",

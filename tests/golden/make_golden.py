@@ -169,11 +169,47 @@ def _exact_cases():
     print("exact", names)
 
 
+def per_query_counters_case(rows: int = 200, ef: int = 192) -> None:
+    """The reference's own work counters query by query: one ``HNSWIndex.search`` per query on the
+    10K mixture graph at ef = 192 (the efSearch of the 1M benchmark's plain operating point), the
+    counters reset before each call. ``search_mix10k_counters.npz``."""
+    import tempfile
+
+    from hnsw_engine import HNSWIndex
+
+    from hnsw_engine_b200.graphs import graph_dir, stored_vectors
+
+    src = graph_dir("mix10k")
+    with tempfile.TemporaryDirectory() as tmp:  # the graph directory ships without vectors.npy
+        for f in src.iterdir():
+            if f.is_file():
+                (Path(tmp) / f.name).symlink_to(f)
+        if not (src / "vectors.npy").is_file():
+            np.save(Path(tmp) / "vectors.npy", stored_vectors("mix10k"))
+        index = HNSWIndex.load_native(tmp, mmap=False)
+    q = workload_queries("mix10k")[:rows]
+    ids = np.empty((rows, 10), np.int64)
+    dists = np.empty((rows, 10), np.float64)
+    ctr = np.empty((rows, 2), np.int64)
+    for r in range(rows):
+        index.reset_counters()
+        ids[r], dists[r] = index.search(q[r], k=10, ef=ef)
+        st = index.stats()
+        ctr[r] = (st.distance_computations, st.hops)
+    np.savez_compressed(HERE / "search_mix10k_counters.npz", queries=q, ef=np.int64(ef), ids=ids,
+                        dists=dists, counters=ctr)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference-src", required=True)
+    parser.add_argument("--only", choices=("per_query_counters",), default=None,
+                        help="write only this fixture")
     args = parser.parse_args()
     sys.path.insert(0, args.reference_src)
+    if args.only == "per_query_counters":
+        per_query_counters_case()
+        return
     from hnsw_engine import GraphState, HNSWIndex
     from hnsw_engine.synthetic import clustered, gaussian, small_integers
 
@@ -247,6 +283,7 @@ def main() -> None:
         _quant_case(idx, f"cont_{metric}", queries, 10, 40, (0, 50))
 
     _exact_cases()
+    per_query_counters_case()
 
 
 if __name__ == "__main__":

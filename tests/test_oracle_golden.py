@@ -93,3 +93,20 @@ def test_oracle_epoch_and_threads_do_not_change_results() -> None:
     b = cpu.search_batch(arrays, ep, ml, case["queries"], 10, 50, "l2", threads=8)
     for x, y in zip(a, b, strict=True):
         np.testing.assert_array_equal(x, y)
+
+
+def test_port_does_the_reference_work_query_by_query() -> None:
+    """The CPU restatement timed as the reference arm and the CPU baseline does exactly the
+    reference's work: per query, the same distance computations and hops as the reference's own
+    counters (one ``HNSWIndex.search`` per query at ef = 192, the plain operating point of the 1M
+    benchmark), and the same results. Equal work is what makes its speed stand for the reference's."""
+    from conftest import mix10k_arrays
+    from oracle import cpu
+
+    case = load_golden("search_mix10k_counters")
+    arrays, ep, ml = mix10k_arrays()
+    ids, dists, ctr = cpu.search_batch(arrays, ep, ml, case["queries"], 10, int(case["ef"]), "l2",
+                                       threads=4)
+    np.testing.assert_array_equal(ctr, case["counters"])
+    np.testing.assert_array_equal(ids, case["ids"])
+    np.testing.assert_array_equal(dists, case["dists"])
