@@ -82,6 +82,15 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_LANE_ROWS
 #define HB_LANE_ROWS 1
 #endif
+// Byte rows of one lane per neighbour: staged into shared memory by cp.async (no registers held
+// while the visited marks resolve) instead of loaded into registers.
+#ifndef HB_STAGE_ROWS
+#define HB_STAGE_ROWS 0
+#endif
+// Batched admission: one pass over the chunk's candidates builds each lane's "below me" masks.
+#ifndef HB_ADMIT_MASKS
+#define HB_ADMIT_MASKS 0
+#endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
 #define HB_PROF_DECL unsigned long long hb_t = clock64();
@@ -199,13 +208,18 @@ __host__ __device__ inline int result_slots(int ef_cap) { return ef_cap + 33; }
 // two_ids: the graph is stored in an internal node order, so results keep internal ids next to
 // the original ones (otherwise the two are the same array).
 __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filtered, int s_cap,
-                                                  int k_rerank, bool two_ids) {
-    size_t b = al16(size_t(result_slots(ef_cap)) * 8) +
+                                                  int k_rerank, bool two_ids, int stage = 0) {
+    size_t b = al16(size_t(stage)) + al16(size_t(result_slots(ef_cap)) * 8) +
                (two_ids ? 2 : 1) * al16(size_t(result_slots(ef_cap)) * 4) + al16(size_t(dim) * 8) +
                al16(size_t(dim) * 4) + al16(size_t(dim));
     if (filtered) b += al16(size_t(s_cap + 1) * 8) + (two_ids ? 2 : 1) * al16(size_t(s_cap + 1) * 4);
     if (k_rerank > 0) b += al16(size_t(k_rerank + 1) * 8) + al16(size_t(k_rerank + 1) * 4);
     return b;
+}
+
+// Shared-memory staging of gathered byte rows (bytes per warp: one row per lane), or 0.
+__host__ __device__ inline int stage_bytes(int mode, int lane_rows, int dim) {
+    return (HB_STAGE_ROWS && mode == 2 && lane_rows && (dim & 15) == 0 && dim <= 128) ? 32 * dim : 0;
 }
 
 // D: the type of the result and candidate distances (Rd, Sd, spd). Byte searches use float --
@@ -239,6 +253,7 @@ struct CtxT {
     int32_t status;          // uniform across the warp
     int32_t q;               // query row
     bool lane_rows;          // byte rows fit one lane (dim a multiple of 16, at most 128)
+    unsigned char *stage;    // this warp's row staging (one row per lane), or NULL
 #ifdef HB_PROFILE
     unsigned long long prof[8];  // cycles per phase of this warp's current query
 #endif
@@ -749,12 +764,85 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, 
     return um;
 }
 
+__device__ __forceinline__ void cp_async16(const void *smem_dst, const void *gmem_src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
+                 "l"(gmem_src)
+                 : "memory");
+}
+
+// mark_score_lane_rows with the rows staged in shared memory: each lane copies its neighbour's row
+// into its own staging slot with 16-byte cp.async (16-byte chunk t of lane l lands at chunk
+// t ^ (l & 7) of the slot, so the later reads of a quarter-warp hit distinct banks), resolves the
+// visited marks while the copies fly, waits for its own copies, then sums from shared memory.
+// Each lane reads only what it copied, so no warp barrier is needed. Same integers as the register
+// version.
+template <class Cx>
+__device__ __forceinline__ uint32_t mark_score_lane_rows_staged(const SearchParams &P, Cx &C,
+                                                                int32_t e, int log2, int &vis_count,
+                                                                typename Cx::dist_t &dj) {
+    using D = typename Cx::dist_t;
+    const int v4 = P.dim >> 4;
+    const int sw = v4 == 8 ? (C.lane & 7) : 0;
+    unsigned char *mine = C.stage + C.lane * P.dim;
+    if (e >= 0) {
+        const unsigned char *row = P.rows8 + int64_t(e) * P.dim;
+#pragma unroll
+        for (int t = 0; t < 8; t++)
+            if (t < v4) cp_async16(mine + ((t ^ sw) << 4), row + (t << 4));
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    dj = D(0);
+    if ((um >> C.lane) & 1u) {
+        const uint4 *qv = reinterpret_cast<const uint4 *>(C.q4);
+        const uint4 *xs = reinterpret_cast<const uint4 *>(mine);
+        uint32_t acc = 0u;
+        if (P.metric == HNSW_B200_L2) {
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                if (t < v4) {
+                    const uint4 q = qv[t];
+                    const uint4 x = xs[t ^ sw];
+                    uint32_t d = __vabsdiffu4(x.x, q.x);
+                    acc = __dp4a(d, d, acc);
+                    d = __vabsdiffu4(x.y, q.y);
+                    acc = __dp4a(d, d, acc);
+                    d = __vabsdiffu4(x.z, q.z);
+                    acc = __dp4a(d, d, acc);
+                    d = __vabsdiffu4(x.w, q.w);
+                    acc = __dp4a(d, d, acc);
+                }
+            }
+            dj = D(acc);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                if (t < v4) {
+                    const uint4 q = qv[t];
+                    const uint4 x = xs[t ^ sw];
+                    acc = __dp4a(x.x, q.x, acc);
+                    acc = __dp4a(x.y, q.y, acc);
+                    acc = __dp4a(x.z, q.z, acc);
+                    acc = __dp4a(x.w, q.w, acc);
+                }
+            }
+            dj = -D(acc);
+        }
+    }
+    return um;
+}
+
 // Mark a chunk visited and score its new neighbours (lane j of the returned mask gets dj).
 template <int MODE, bool U8, class Cx>
 __device__ __forceinline__ uint32_t mark_and_score(const SearchParams &P, Cx &C, int32_t e, int log2,
                                                    int &vis_count, typename Cx::dist_t &dj) {
-    if (MODE == MODE_BYTES && HB_LANE_ROWS && C.lane_rows)
+    if (MODE == MODE_BYTES && HB_LANE_ROWS && C.lane_rows) {
+        // stage_bytes() gives every lane-row search of a byte kernel its staging slot
+        if constexpr (HB_STAGE_ROWS) return mark_score_lane_rows_staged(P, C, e, log2, vis_count, dj);
         return mark_score_lane_rows(P, C, e, log2, vis_count, dj);
+    }
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
     score_chunk<MODE, U8>(P, C, e, um, dj);
     return um;
@@ -934,6 +1022,26 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
             eq_lt += (C.Ri[i] & ID_MASK) < eo;
         }
     }
+#if HB_ADMIT_MASKS
+    // One pass over the candidates: the ones below mine by (distance, id), and the earlier ones at
+    // or below my distance, as lane masks.
+    uint32_t ltm = 0u, plem = 0u;
+    for (uint32_t m = cm; m;) {
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        const D di = __shfl_sync(FULL, dj, i);
+        const int32_t ii = __shfl_sync(FULL, eo, i);
+        const uint32_t bit = 1u << i;
+        ltm |= (di < dj || (di == dj && ii < eo)) ? bit : 0u;
+        plem |= (i < lane && di <= dj) ? bit : 0u;
+    }
+    const bool adm = inc && lo + n_eq + __popc(plem) < ef;
+    const uint32_t A = __ballot_sync(FULL, adm);
+    if (!A) return;
+    // admitted pairs below mine: all of them, and earlier ones
+    const int rank_a = __popc(ltm & A);
+    const int rank_prev = __popc(ltm & A & ((1u << lane) - 1u));
+#else
     int prev_le = 0;  // earlier candidates of the chunk at or below dj
     for (uint32_t m = cm; m;) {
         const int i = __ffs(m) - 1;
@@ -954,6 +1062,7 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
         rank_a += lt;
         rank_prev += (lt && i < lane);
     }
+#endif
     const int pos_r0 = lo + eq_lt;  // entries of R0 below (dj, e)
     const int fpos = pos_r0 + rank_a;
     churn += __popc(__ballot_sync(FULL, adm && pos_r0 + rank_prev < P.k));
@@ -1423,11 +1532,14 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
     const int lane = threadIdx.x & 31;
     const bool rerank = P.rerank_queries != nullptr;
     const bool two_ids = P.node_ids != nullptr;
-    const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids);
+    const int stage = stage_bytes(MODE, P.lane_rows, P.dim);
+    const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids, stage);
     unsigned char *p = smem + size_t(warp) * wb;
     using D = std::conditional_t<MODE == MODE_BYTES, float, double>;
     CtxT<D> C;
     C.lane = lane;
+    C.stage = stage ? p : nullptr;
+    p += al16(size_t(stage));
     C.Rd = reinterpret_cast<D *>(p);  // 8 bytes a slot are reserved either way
     p += al16(size_t(result_slots(P.ef_cap)) * 8);
     C.Ri = reinterpret_cast<int32_t *>(p);
@@ -1848,7 +1960,12 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
     const int s_cap = 256;
-    const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr, g.node_ids != nullptr);
+    // One lane per neighbour's row: a win unless the filter is very selective, where most rows it
+    // would fetch early belong to neighbours already visited.
+    const double p = filt ? std::max(double(a->allowed_fraction), 1.0 / double(g.n)) : 1.0;
+    const int lane_rows = (!filt || p >= 0.05) ? 1 : 0;
+    const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr, g.node_ids != nullptr,
+                                      stage_bytes(mode, lane_rows, g.dim));
     const bool use_mlp = a->stop_mlp != nullptr && !filt;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (a->trace_feat && (!a->trace_dk || !a->trace_count || !a->trace_hops || a->trace_cap < 1))
@@ -1863,7 +1980,6 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
 
     // Scratch sizing from the expected work per query: visits grow about linearly with ef and
     // inversely with the share of allowed nodes.
-    const double p = filt ? std::max(double(a->allowed_fraction), 1.0 / double(g.n)) : 1.0;
     const double est = std::min(double(g.n) + 64.0, (12.0 * ef_cap + 256.0) / p);
     int vis_log2 = std::max(8, ilog2_ceil(int64_t(2.0 * est)));
     int vis_up_log2 = 10;
@@ -1924,9 +2040,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     P.cell_cost = a->cell_cost;
     P.n_cells = a->n_cells;
     P.trace_k = 16;
-    // One lane per neighbour's row: a win unless the filter is very selective, where most rows it
-    // would fetch early belong to neighbours already visited.
-    P.lane_rows = (!filt || p >= 0.05) ? 1 : 0;
+    P.lane_rows = lane_rows;
 
     int32_t n_work = nq;
     const int32_t *qlist = nullptr;
@@ -2089,7 +2203,8 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
                          : (a->dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64);
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
-    const size_t wb = warp_smem_bytes(ef_cap, g.dim, false, 256, krr, g.node_ids != nullptr);
+    const size_t wb = warp_smem_bytes(ef_cap, g.dim, false, 256, krr, g.node_ids != nullptr,
+                                      stage_bytes(mode, 1, g.dim));
     const bool use_mlp = a->stop_mlp != nullptr;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (smem_block > 227 * 1024) return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory");
