@@ -78,6 +78,7 @@ class SearchArgs(ctypes.Structure):
         ("cells", ctypes.c_void_p),
         ("cell_cost", ctypes.c_void_p),
         ("n_cells", ctypes.c_int32),
+        ("kernel_config", ctypes.c_int32),
     ]
 
 
@@ -154,6 +155,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                                                 ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p,
                                                 ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_version": (ctypes.c_char_p, []),
+    "hnsw_b200_kernel_configs": (ctypes.c_int32, [ctypes.c_int32]),
+    "hnsw_b200_kernel_config_name": (ctypes.c_char_p, [ctypes.c_int32, ctypes.c_int32]),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -71,10 +71,13 @@ struct FilterParams {
     const float *qq;       // |q|^2 per query (l2)
     const float *xx;       // |x|^2 per row (l2)
     const float *thr;      // per query: tau + margin (+inf in pass one)
-    float *cand_val;       // (nq, cap) approximate distances
-    int32_t *cand_id;      // (nq, cap) row ids
-    int32_t *cand_cnt;     // (nq,) appended counts (may exceed cap: overflow)
-    int32_t cap;
+    // Candidates in segments: every epilogue thread of the grid owns one segment of its query's
+    // list (segment = row split x epilogue part), so appends need no atomics. Segment s of query q
+    // starts at (q * nseg + s) * cap.
+    float *cand_val;       // (nq, nseg, cap) approximate distances
+    int32_t *cand_id;      // (nq, nseg, cap) row ids
+    int32_t *cand_cnt;     // (nq, nseg) appended counts (may exceed cap: overflow)
+    int32_t cap;           // entries per segment
     int32_t block_min;     // 1: append only the minimum of each 32-row block (the threshold pass)
     int32_t *err;          // nonzero: a bounded wait expired
 };
@@ -328,8 +331,11 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         const bool qvalid = q < p.nq;
         const float qq = qvalid ? p.qq[q] : 0.f;
         const float thr = qvalid ? p.thr[q] : -INFINITY;
-        float *cv = p.cand_val + int64_t(qvalid ? q : 0) * p.cap;
-        int32_t *ci = p.cand_id + int64_t(qvalid ? q : 0) * p.cap;
+        const int nseg = int(gridDim.y) * EPI_PER_QUARTER;
+        const int64_t seg = int64_t(qvalid ? q : 0) * nseg + int64_t(blockIdx.y) * EPI_PER_QUARTER + part;
+        float *cv = p.cand_val + seg * p.cap;
+        int32_t *ci = p.cand_id + seg * p.cap;
+        int cnt = 0;  // this thread's appends (its own segment: no atomics)
         const bool l2 = p.metric == HNSW_B200_L2;
         const bool cosine = p.metric == HNSW_B200_COSINE;
         for (int lt = 0; lt < ntiles; lt++) {
@@ -400,23 +406,21 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                     for (int j = 0; j < 32; j++)
                         if ((keep >> j) & 1u) mn = fminf(mn, v[j]);
                     if (keep && qvalid) {
-                        const int o = atomicAdd(p.cand_cnt + q, 1);
-                        if (o < p.cap) {
-                            cv[o] = mn;
-                            ci[o] = col0;
+                        if (cnt < p.cap) {
+                            cv[cnt] = mn;
+                            ci[cnt] = col0;
                         }
+                        cnt++;
                     }
                 } else if (keep && qvalid) {
-                    const int cnt = __popc(keep);
-                    int o = atomicAdd(p.cand_cnt + q, cnt);
 #pragma unroll
                     for (int j = 0; j < 32; j++) {  // static indices keep v[] in registers
                         if ((keep >> j) & 1u) {
-                            if (o < p.cap) {
-                                cv[o] = v[j];
-                                ci[o] = col0 + j;
+                            if (cnt < p.cap) {
+                                cv[cnt] = v[j];
+                                ci[cnt] = col0 + j;
                             }
-                            o++;
+                            cnt++;
                         }
                     }
                 }
@@ -425,6 +429,7 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(tempty + b);
         }
+        if (qvalid) p.cand_cnt[seg] = cnt;
     }
     __syncthreads();
     if (warp == 2) {
@@ -497,15 +502,17 @@ __device__ __forceinline__ float funkey(uint32_t k) {
 
 // One block of 256 threads per query: tau[q] = k-th smallest of the candidate values (or +inf if
 // fewer than k), then out_thr[q] = tau + margin[q].
-__global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32_t cap, int32_t nq,
-                           int32_t k, const float *margin, float *out_thr, float *out_tau) {
+__global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32_t cap, int32_t nseg,
+                           int32_t nq, int32_t k, const float *margin, float *out_thr, float *out_tau) {
     __shared__ uint32_t hist[256];
     __shared__ uint32_t wsum[8];  // per-warp bin totals (blockDim.x == 256)
     __shared__ uint32_t s_prefix, s_rank;
     const int q = blockIdx.x;
     if (q >= nq) return;
-    const int m = min(cand_cnt[q], cap);
-    const float *v = cand_val + int64_t(q) * cap;
+    const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
+    int m = 0;
+    for (int sg = 0; sg < nseg; sg++) m += min(cnt[sg], cap);
+    const float *v = cand_val + int64_t(q) * nseg * cap;
     if (m < k) {
         if (threadIdx.x == 0) {
             out_tau[q] = INFINITY;
@@ -518,9 +525,12 @@ __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32
         for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
         __syncthreads();
         const uint32_t hmask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
-        for (int i = threadIdx.x; i < m; i += blockDim.x) {
-            const uint32_t key = fkey(v[i]);
-            if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        for (int sg = 0; sg < nseg; sg++) {
+            const int ms = min(cnt[sg], cap);
+            for (int i = threadIdx.x; i < ms; i += blockDim.x) {
+                const uint32_t key = fkey(v[int64_t(sg) * cap + i]);
+                if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+            }
         }
         __syncthreads();
         // The bucket holding the rank-th key: the bin whose counts before it are below rank and
@@ -565,8 +575,8 @@ template <typename T>
 __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq, int32_t k,
                             int32_t metric, const double *xnorm, const double *qnorm,
                             const float *cand_val, const int32_t *cand_id, const int32_t *cand_cnt,
-                            int32_t cap, const float *thr, int64_t *out_ids, double *out_d,
-                            unsigned long long *err_max) {
+                            int32_t cap, int32_t nseg, const float *thr, int64_t *out_ids,
+                            double *out_d, unsigned long long *err_max) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warps = blockDim.x >> 5;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -575,17 +585,19 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
     int32_t *Ai = reinterpret_cast<int32_t *>(reinterpret_cast<double *>(sm) + size_t(warps) * (k + 1)) +
                   size_t(w) * (k + 1);
     if (q >= nq) return;
-    const int m = min(cand_cnt[q], cap);
     const float t = thr[q];
     const T *qv = queries + int64_t(q) * dim;
     const double qn = qnorm[q];
     int a = 0;
     double err = 0.0;  // largest |filter value - exact distance| over this lane's survivors
+    for (int sg = 0; sg < nseg; sg++) {
+    const int m = min(cand_cnt[int64_t(q) * nseg + sg], cap);
+    const int64_t sb = (int64_t(q) * nseg + sg) * cap;
     for (int base = 0; base < m; base += 32) {
         const int i = base + lane;
-        const float approx = i < m ? cand_val[int64_t(q) * cap + i] : INFINITY;
+        const float approx = i < m ? cand_val[sb + i] : INFINITY;
         bool has = i < m && approx <= t;
-        int32_t id = has ? cand_id[int64_t(q) * cap + i] : -1;
+        int32_t id = has ? cand_id[sb + i] : -1;
         double d = INFINITY;
         if (has) {
             const T *x = data + int64_t(id) * dim;
@@ -640,6 +652,7 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
             a = min(a + 1, k);
         }
     }
+    }
     for (int r = lane; r < k; r += 32) {
         out_ids[int64_t(q) * k + r] = r < a ? int64_t(Ai[r]) : -1;
         out_d[int64_t(q) * k + r] = r < a ? Ad[r] : INFINITY;
@@ -650,6 +663,26 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) eb = max(eb, __shfl_xor_sync(0xffffffffu, eb, o));
     if (lane == 0 && eb) atomicMax(err_max, eb);
+}
+
+// Largest and total of the segment counts (overflow check and the candidate total).
+__global__ void count_stats(const int32_t *cnt, int64_t len, unsigned long long *out) {
+    unsigned long long mx = 0, sum = 0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < len;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const unsigned long long c = static_cast<unsigned long long>(cnt[i]);
+        mx = max(mx, c);
+        sum += c;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, mx);
+        atomicAdd(out + 1, sum);
+    }
 }
 
 // Error bound of the filter arithmetic and the per-query margins (2 e_q).
@@ -737,8 +770,15 @@ struct Scratch {
 
 size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Candidate lists take about CAND_BYTES of scratch: (queries per chunk) x cap x 8 bytes.
+// Candidate lists take at most CAND_BYTES of scratch: (query, segment) pairs x cap x 8 bytes.
 constexpr int64_t CAND_BYTES = int64_t(4) << 30;
+// Pass two keeps about k n / prefix rows per query: tau is the k-th smallest of the prefix's 32-row
+// block minima, a loose upper bound of the k-th distance (3,244 per query measured for k = 100 on the
+// 1M x 128 mixture, against 3,100 for k n / prefix). Lists are sized for EXPECT_FACTOR times that.
+#ifndef HB_EXPECT_FACTOR
+#define HB_EXPECT_FACTOR 2
+#endif
+constexpr int64_t EXPECT_FACTOR = HB_EXPECT_FACTOR;
 
 // One attempt at the whole batch with candidate lists of at least cap_min entries. Returns
 // HNSW_B200_ERETRY with *cap_needed set when a query's candidates outgrew its list (many rows
@@ -757,19 +797,45 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 
-    // Candidate capacity: pass one keeps every row of its prefix; pass two about k * n / prefix.
+    // Split geometry of a pass over `rows` rows for a chunk of nqc queries: the rows are split so
+    // that the chunk's query tiles fill the GPU (about four CTAs per SM).
+    struct Geo {
+        int tps, splits;
+    };
+    auto geo = [&](int64_t nqc, int64_t rows) {
+        const int qt = int((nqc + BM - 1) / BM);
+        const int tiles = int((rows + BN - 1) / BN);
+        const int want = std::max(1, (4 * sms + qt - 1) / qt);
+        Geo g;
+        g.tps = std::max(1, (tiles + want - 1) / want);
+        g.splits = (tiles + g.tps - 1) / g.tps;
+        return g;
+    };
+    // Pass one keeps the minimum of every 32-row block of a prefix (every row when the prefix has
+    // fewer than k blocks); pass two keeps the rows within tau + margin, about EXPECT_FACTOR k n /
+    // prefix of them. Each epilogue thread appends to its own segment of the query's list: at most
+    // 3 (block minima) or 96 (rows) entries per tile in pass one; pass two's segments are sized for
+    // three times their expected share (an overflow re-runs the call with longer segments).
     const int64_t prefix = std::min<int64_t>(n, std::max<int64_t>(int64_t(64) * k, 32768));
-    const int64_t qb_max = std::min<int64_t>(nq_all, 8192);
-    int64_t cap = std::max<int64_t>(
-        prefix, std::min<int64_t>(n, 24 * int64_t(k) * (n / std::max<int64_t>(prefix, 1)) + 4096));
-    cap = std::min<int64_t>(cap, std::max<int64_t>(prefix, CAND_BYTES / (8 * qb_max)));
-    cap = std::max<int64_t>(cap, std::min<int64_t>(cap_min, n));
-    // Queries per chunk: up to 8192, fewer when a retry needs longer candidate lists.
-    int64_t QB = qb_max;
-    if (QB * cap * 8 > CAND_BYTES)
-        QB = std::min<int64_t>(qb_max, std::max<int64_t>(BM, CAND_BYTES / (8 * cap) / BM * BM));
+    const bool block_min = (prefix + 31) / 32 >= k;
+    const int64_t expect2 = EXPECT_FACTOR * int64_t(k) * ((n + prefix - 1) / prefix) + int64_t(k);
+    int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
+    int64_t cap = 0, slots = 0;                      // entries per segment; (query, segment) pairs
+    for (;;) {
+        cap = std::min<int64_t>(cap_min, n);
+        slots = 0;
+        const int64_t last = nq_all % QB ? nq_all % QB : QB;
+        for (int64_t nqc : {QB, last}) {
+            const Geo g1 = geo(nqc, prefix), g2 = geo(nqc, n);
+            const int64_t nseg2 = int64_t(g2.splits) * EPI_PER_QUARTER;
+            cap = std::max<int64_t>(cap, int64_t(block_min ? 3 : 96) * g1.tps);
+            cap = std::max<int64_t>(cap, (3 * expect2 + nseg2 - 1) / nseg2 + 32);
+            slots = std::max<int64_t>(slots, nqc * std::max(g1.splits, g2.splits) * EPI_PER_QUARTER);
+        }
+        if (slots * cap * 8 <= CAND_BYTES || QB <= BM) break;
+        QB = std::max<int64_t>(BM, QB / 2 / BM * BM);  // longer lists: fewer queries per chunk
+    }
     const int64_t q_pad = (QB + BM - 1) / BM * BM;
-
     static thread_local Scratch buf;
     size_t off = 0;
     auto carve = [&](size_t bytes) {
@@ -786,9 +852,10 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     const size_t o_mg = carve(size_t(QB) * 4);
     const size_t o_th = carve(size_t(QB) * 4);
     const size_t o_tau = carve(size_t(QB) * 4);
-    const size_t o_cnt = carve(size_t(QB) * 4);
-    const size_t o_cv = carve(size_t(QB) * cap * 4);
-    const size_t o_ci = carve(size_t(QB) * cap * 4);
+    const size_t o_cnt = carve(size_t(slots) * 4);
+    const size_t o_cv = carve(size_t(slots) * cap * 4);
+    const size_t o_ci = carve(size_t(slots) * cap * 4);
+    const size_t o_cs = carve(16);
     const size_t o_err = carve(16);
     const size_t o_mx = carve(16);
     const size_t o_fe = carve(16);
@@ -840,7 +907,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     auto *ferr = reinterpret_cast<unsigned long long *>(B + o_fe);  // measured filter error (bits)
     XT(cudaMemsetAsync(ferr, 0, 8, s));
     std::vector<float> inf(static_cast<size_t>(QB), INFINITY);
-    std::vector<int32_t> hc(static_cast<size_t>(QB));
+    auto *cstat = reinterpret_cast<unsigned long long *>(B + o_cs);  // largest and total count
     double max_margin = 0.0;
     int64_t total_cand = 0;
 
@@ -854,11 +921,11 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         launches += 2;
         // Query tiles of this chunk only (the last chunk may be short), rows split to fill the GPU.
         const int qt_chunk = int((nq + BM - 1) / BM);
-        auto run_filter = [&](int64_t row_end, bool block_min) -> int {
-            const int tiles = int((row_end + BN - 1) / BN);
-            const int want_splits = std::max(1, (4 * sms + qt_chunk - 1) / qt_chunk);
-            const int tps = std::max(1, (tiles + want_splits - 1) / want_splits);
-            const int splits = (tiles + tps - 1) / tps;
+        int nseg = 0;  // segments per query of the last pass run
+        auto run_filter = [&](int64_t row_end, bool bmin) -> int {
+            const Geo gg = geo(nq, row_end);
+            const int tps = gg.tps, splits = gg.splits;
+            nseg = splits * EPI_PER_QUARTER;
             FilterParams fp;
             fp.nq = int32_t(nq);
             fp.row_begin = 0;
@@ -873,9 +940,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
             fp.cand_id = ci;
             fp.cand_cnt = cnt;
             fp.cap = int32_t(cap);
-            fp.block_min = block_min ? 1 : 0;
+            fp.block_min = bmin ? 1 : 0;
             fp.err = err;
-            XT(cudaMemsetAsync(cnt, 0, size_t(nq) * 4, s));
             knn_filter_kernel<<<dim3(qt_chunk, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
             XT(cudaGetLastError());
             launches++;
@@ -884,29 +950,34 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         // Pass one: the prefix rows with no threshold give tau (an upper bound of the k-th).
         XT(cudaMemcpyAsync(th, inf.data(), size_t(nq) * 4, cudaMemcpyHostToDevice, s));
         // One candidate per 32-row block suffices while the prefix has at least k blocks.
-        if (int rc = run_filter(prefix, (prefix + 31) / 32 >= k)) return rc;
-        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nq), k, mg, th, tau);
+        if (int rc = run_filter(prefix, block_min)) return rc;
+        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg,
+                                           th, tau);
         // Pass two: every row against tau + margin.
         if (int rc = run_filter(n, false)) return rc;
+        XT(cudaMemsetAsync(cstat, 0, 16, s));
+        count_stats<<<int(std::min<int64_t>(1024, (nq * nseg + 255) / 256)), 256, 0, s>>>(
+            cnt, nq * nseg, cstat);
+        XT(cudaGetLastError());
+        launches++;
         int32_t herr[4];
-        XT(cudaMemcpyAsync(hc.data(), cnt, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
+        unsigned long long hst[2];
+        XT(cudaMemcpyAsync(hst, cstat, 16, cudaMemcpyDeviceToHost, s));
         XT(cudaMemcpyAsync(herr, err, 16, cudaMemcpyDeviceToHost, s));
         XT(cudaStreamSynchronize(s));
         if (herr[0]) return fail(HNSW_B200_ECUDA, "exact knn: a bounded wait expired in the filter kernel");
-        int32_t worst = 0;
-        for (int64_t i = 0; i < nq; i++) {
-            worst = std::max(worst, hc[size_t(i)]);
-            total_cand += hc[size_t(i)];
-        }
+        const int64_t worst = int64_t(hst[0]);
+        total_cand += int64_t(hst[1]);
         if (worst > cap) {
             *cap_needed = worst;
             return fail(HNSW_B200_ERETRY, "exact knn: candidate buffer overflow (" + std::to_string(worst) +
                                               " > " + std::to_string(cap) + ")");
         }
         // The k-th smallest candidate is the global k-th approximate distance: final threshold.
-        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nq), k, mg, th, tau);
+        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg,
+                                           th, tau);
         rerank_topk<T><<<int((nq + wpb - 1) / wpb), wpb * 32, rsm, s>>>(
-            X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), th,
+            X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), int32_t(nseg), th,
             a->out_ids + q0 * k, a->out_dists + q0 * k, ferr);
         XT(cudaGetLastError());
         launches += 3;

@@ -74,22 +74,15 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_BATCH_ADMIT
 #define HB_BATCH_ADMIT 1
 #endif
-// Unfiltered layer 0 visited set: 0 the per-slot bitmap, 1 a per-slot open-addressing hash.
-#ifndef HB_L0_HASH
-#define HB_L0_HASH 0
-#endif
 // Byte rows of at most 128 bytes: one lane per neighbour, row loads issued before the visited marks.
 #ifndef HB_LANE_ROWS
 #define HB_LANE_ROWS 1
 #endif
-// Byte rows of one lane per neighbour: staged into shared memory by cp.async (no registers held
-// while the visited marks resolve) instead of loaded into registers.
-#ifndef HB_STAGE_ROWS
-#define HB_STAGE_ROWS 0
-#endif
-// Batched admission: one pass over the chunk's candidates builds each lane's "below me" masks.
+// Batched admission: one pass over the chunk's candidates builds each lane's "below me" masks
+// (3.5% faster than counting over the admitted set in a second pass: 3.45 -> 3.33 ms at ef = 192 on
+// the 1M mixture, identical results).
 #ifndef HB_ADMIT_MASKS
-#define HB_ADMIT_MASKS 0
+#define HB_ADMIT_MASKS 1
 #endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
@@ -107,17 +100,32 @@ __device__ unsigned long long hb_prof[8];
     } while (0)
 #endif
 
-template <int MODE>
-struct MinBlocks {
-    // Filtered byte searches: 5 blocks (96 registers) against 6 (80 registers, spilling 184
-    // bytes) measured 4.18 against 4.72 ms at Bernoulli p = 0.5 and 17.2 against 18.9 ms at
-    // p = 0.1 on the 1M mixture (float32 candidates).
-    template <bool FILT>
-    static constexpr int of() {
-        return MODE == 2 ? (FILT ? HB_MINB_BYTES_FILT : HB_MINB_BYTES)
-                         : (MODE == 1 ? HB_MINB_EXACT : HB_MINB_F64);
-    }
-};
+// Kernel configurations among which the autotuner picks, for the byte kernels (the other modes
+// build configuration 0 only): the resident blocks per SM requested from the compiler (which caps
+// the registers per thread), the gathered rows of one lane per neighbour held in registers or
+// staged in shared memory by cp.async, and the unfiltered layer-0 visited set as the per-slot
+// bitmap or a per-slot open-addressing hash. Every configuration gives the same results.
+constexpr int N_CONFIGS = 4;
+__host__ __device__ constexpr int cfg_blocks(int c) { return c == 1 ? 4 : 5; }
+__host__ __device__ constexpr bool cfg_stage(int c) { return c == 2; }
+__host__ __device__ constexpr bool cfg_hash(int c) { return c == 3; }
+inline const char *cfg_name(int c) {
+    return c == 0 ? "bitmap, rows in registers, 5 blocks/SM"
+                  : c == 1 ? "bitmap, rows in registers, 4 blocks/SM"
+                           : c == 2 ? "bitmap, rows staged by cp.async, 5 blocks/SM"
+                                    : "hash, rows in registers, 5 blocks/SM";
+}
+// Configurations built for a mode (byte kernels: all; the others: configuration 0).
+__host__ __device__ constexpr int configs_of(int mode) { return mode == 2 ? N_CONFIGS : 1; }
+
+// Resident blocks per SM requested for a kernel. Filtered byte searches: 5 blocks (96 registers)
+// against 6 (80 registers, spilling 184 bytes) measured 4.18 against 4.72 ms at Bernoulli p = 0.5
+// and 17.2 against 18.9 ms at p = 0.1 on the 1M mixture (float32 candidates).
+template <int MODE, bool FILT, int CFG>
+constexpr int min_blocks() {
+    if (MODE == 2) return CFG == 0 ? (FILT ? HB_MINB_BYTES_FILT : HB_MINB_BYTES) : cfg_blocks(CFG);
+    return MODE == 1 ? HB_MINB_EXACT : HB_MINB_F64;
+}
 
 enum : int32_t { ST_VISITED = 1, ST_TIES = 2, ST_SPILL = 4 };
 enum : int { MODE_F64 = 0, MODE_EXACT = 1, MODE_BYTES = 2 };
@@ -218,8 +226,8 @@ __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filt
 }
 
 // Shared-memory staging of gathered byte rows (bytes per warp: one row per lane), or 0.
-__host__ __device__ inline int stage_bytes(int mode, int lane_rows, int dim) {
-    return (HB_STAGE_ROWS && mode == 2 && lane_rows && (dim & 15) == 0 && dim <= 128) ? 32 * dim : 0;
+__host__ __device__ inline int stage_bytes(int mode, int cfg, int lane_rows, int dim) {
+    return (cfg_stage(cfg) && mode == 2 && lane_rows && (dim & 15) == 0 && dim <= 128) ? 32 * dim : 0;
 }
 
 // D: the type of the result and candidate distances (Rd, Sd, spd). Byte searches use float --
@@ -835,12 +843,12 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows_staged(const SearchPara
 }
 
 // Mark a chunk visited and score its new neighbours (lane j of the returned mask gets dj).
-template <int MODE, bool U8, class Cx>
+template <int MODE, bool U8, int CFG, class Cx>
 __device__ __forceinline__ uint32_t mark_and_score(const SearchParams &P, Cx &C, int32_t e, int log2,
                                                    int &vis_count, typename Cx::dist_t &dj) {
     if (MODE == MODE_BYTES && HB_LANE_ROWS && C.lane_rows) {
         // stage_bytes() gives every lane-row search of a byte kernel its staging slot
-        if constexpr (HB_STAGE_ROWS) return mark_score_lane_rows_staged(P, C, e, log2, vis_count, dj);
+        if constexpr (cfg_stage(CFG)) return mark_score_lane_rows_staged(P, C, e, log2, vis_count, dj);
         return mark_score_lane_rows(P, C, e, log2, vis_count, dj);
     }
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
@@ -1140,11 +1148,11 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
     scan = min(scan, fmin);
 }
 
-template <int MODE, bool U8, class Cx>
+template <int MODE, bool U8, int CFG, class Cx>
 __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, int log2, int &r) {
     using D = typename Cx::dist_t;
     const int lane = C.lane;
-    if (layer > 0 || (HB_L0_HASH && log2 > 0)) {
+    if (layer > 0 || (cfg_hash(CFG) && log2 > 0)) {
         vis_clear(C.vis, log2, lane);
         if (lane == 0) vis_insert(C.vis, log2, C.Rp[0] & ID_MASK);
         __syncwarp();
@@ -1199,7 +1207,7 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
             HB_PROF(2);
             HB_PROF(3);
             D dj;
-            const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
+            const uint32_t um = mark_and_score<MODE, U8, CFG>(P, C, e, log2, vis_count, dj);
 #ifdef HB_PROFILE
             if (__shfl_sync(FULL, dj, 0) == -12345.0) C.status |= 64;  // consume before timing
 #endif
@@ -1416,7 +1424,7 @@ __device__ void cand_refill(const SearchParams &P, Cx &C, CandsT<typename Cx::di
 // numba_engine._search_layer0_filtered (:151-198): results hold allowed nodes only, the worst of
 // an empty result list is +inf, and the search stops only when the results are full and the
 // closest candidate is strictly farther than the worst.
-template <int MODE, bool U8, class Cx>
+template <int MODE, bool U8, int CFG, class Cx>
 __device__ void layer0_filtered(const SearchParams &P, Cx &C, int ef, int log2, double d0,
                                 int32_t e0, int32_t o0, int &r) {
     using D = typename Cx::dist_t;
@@ -1457,7 +1465,7 @@ __device__ void layer0_filtered(const SearchParams &P, Cx &C, int ef, int log2, 
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
             const int32_t eo = e >= 0 ? orig_id(P, e) : -1;
             D dj;
-            const uint32_t um = mark_and_score<MODE, U8>(P, C, e, log2, vis_count, dj);
+            const uint32_t um = mark_and_score<MODE, U8, CFG>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
@@ -1524,15 +1532,15 @@ __device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m) {
 }
 
 // --------------------------------------------------------------------------------------- kernel
-template <int MODE, bool U8, bool FILT>
-__global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>())
+template <int MODE, bool U8, bool FILT, int CFG>
+__global__ void __launch_bounds__(WPB * 32, min_blocks<MODE, FILT, CFG>())
     search_kernel(const SearchParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const bool rerank = P.rerank_queries != nullptr;
     const bool two_ids = P.node_ids != nullptr;
-    const int stage = stage_bytes(MODE, P.lane_rows, P.dim);
+    const int stage = stage_bytes(MODE, CFG, P.lane_rows, P.dim);
     const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids, stage);
     unsigned char *p = smem + size_t(warp) * wb;
     using D = std::conditional_t<MODE == MODE_BYTES, float, double>;
@@ -1647,7 +1655,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
             }
             __syncwarp();
             r = 1;
-            layer_search<MODE, U8>(P, C, layer, 1, P.vis_up_log2, r);
+            layer_search<MODE, U8, CFG>(P, C, layer, 1, P.vis_up_log2, r);
             d0 = C.Rd[0];
             o0 = C.Ri[0] & ID_MASK;
             e0 = C.Rp[0] & ID_MASK;
@@ -1656,7 +1664,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
         const int ef0 = max(__ldg(P.ef + q), P.k_search);
         if (!C.status) {
             if constexpr (FILT) {
-                layer0_filtered<MODE, U8>(P, C, ef0, P.vis_log2, d0, e0, o0, r);
+                layer0_filtered<MODE, U8, CFG>(P, C, ef0, P.vis_log2, d0, e0, o0, r);
             } else {
                 if (lane == 0) {
                     C.Rd[0] = D(d0);
@@ -1665,7 +1673,7 @@ __global__ void __launch_bounds__(WPB * 32, MinBlocks<MODE>::template of<FILT>()
                 }
                 __syncwarp();
                 r = 1;
-                layer_search<MODE, U8>(P, C, 0, ef0, P.vis_log2, r);
+                layer_search<MODE, U8, CFG>(P, C, 0, ef0, P.vis_log2, r);
             }
             bitmap_clear(P, C);
         }
@@ -1789,21 +1797,9 @@ struct Handle {
     std::mutex mu;
 };
 
-template <int MODE, bool U8, bool FILT>
-int launch_one(Handle &h, const SearchParams &P, size_t smem_block, int blocks, cudaStream_t s) {
-    auto kern = search_kernel<MODE, U8, FILT>;
-    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(smem_block)));
-    kern<<<blocks, WPB * 32, smem_block, s>>>(P);
-    CUDA_TRY(cudaGetLastError());
-    h.launches++;
-    return 0;
-}
-
-// Launch of the unfiltered kernel without a handle (the fixed-scratch entry point).
-template <int MODE, bool U8>
-int launch_one_noalloc(const SearchParams &P, size_t smem_block, int blocks, cudaStream_t s) {
-    auto kern = search_kernel<MODE, U8, false>;
+template <int MODE, bool U8, bool FILT, int CFG>
+int launch_one(const SearchParams &P, size_t smem_block, int blocks, cudaStream_t s) {
+    auto kern = search_kernel<MODE, U8, FILT, CFG>;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem_block)));
     kern<<<blocks, WPB * 32, smem_block, s>>>(P);
@@ -1811,26 +1807,33 @@ int launch_one_noalloc(const SearchParams &P, size_t smem_block, int blocks, cud
     return 0;
 }
 
-template <int MODE, bool U8>
-int launch_mode(Handle &h, const SearchParams &P, bool filt, size_t smem_block, int blocks,
-                cudaStream_t s) {
-    return filt ? launch_one<MODE, U8, true>(h, P, smem_block, blocks, s)
-                : launch_one<MODE, U8, false>(h, P, smem_block, blocks, s);
+template <int MODE, bool U8, int CFG>
+int launch_cfg(const SearchParams &P, bool filt, size_t smem_block, int blocks, cudaStream_t s) {
+    return filt ? launch_one<MODE, U8, true, CFG>(P, smem_block, blocks, s)
+                : launch_one<MODE, U8, false, CFG>(P, smem_block, blocks, s);
 }
 
-int dispatch(Handle &h, const SearchParams &P, int mode, bool u8, bool filt, size_t smem_block,
+// One launch of the kernel for (mode, rows, filter, configuration); cfg < configs_of(mode).
+int dispatch(const SearchParams &P, int mode, bool u8, bool filt, int cfg, size_t smem_block,
              int blocks, cudaStream_t s) {
-    if (mode == MODE_BYTES) return launch_mode<MODE_BYTES, true>(h, P, filt, smem_block, blocks, s);
+    if (mode == MODE_BYTES) {
+        switch (cfg) {
+            case 1: return launch_cfg<MODE_BYTES, true, 1>(P, filt, smem_block, blocks, s);
+            case 2: return launch_cfg<MODE_BYTES, true, 2>(P, filt, smem_block, blocks, s);
+            case 3: return launch_cfg<MODE_BYTES, true, 3>(P, filt, smem_block, blocks, s);
+            default: return launch_cfg<MODE_BYTES, true, 0>(P, filt, smem_block, blocks, s);
+        }
+    }
     if (mode == MODE_EXACT)
-        return u8 ? launch_mode<MODE_EXACT, true>(h, P, filt, smem_block, blocks, s)
-                  : launch_mode<MODE_EXACT, false>(h, P, filt, smem_block, blocks, s);
-    return u8 ? launch_mode<MODE_F64, true>(h, P, filt, smem_block, blocks, s)
-              : launch_mode<MODE_F64, false>(h, P, filt, smem_block, blocks, s);
+        return u8 ? launch_cfg<MODE_EXACT, true, 0>(P, filt, smem_block, blocks, s)
+                  : launch_cfg<MODE_EXACT, false, 0>(P, filt, smem_block, blocks, s);
+    return u8 ? launch_cfg<MODE_F64, true, 0>(P, filt, smem_block, blocks, s)
+              : launch_cfg<MODE_F64, false, 0>(P, filt, smem_block, blocks, s);
 }
 
-template <int MODE, bool U8, bool FILT>
+template <int MODE, bool U8, bool FILT, int CFG>
 int occupancy_of(size_t smem_block, int *blocks_per_sm) {
-    auto kern = search_kernel<MODE, U8, FILT>;
+    auto kern = search_kernel<MODE, U8, FILT, CFG>;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem_block)));
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, WPB * 32,
@@ -1838,20 +1841,26 @@ int occupancy_of(size_t smem_block, int *blocks_per_sm) {
     return 0;
 }
 
-int occupancy(int mode, bool u8, bool filt, size_t smem_block, int *bps) {
-    if (mode == MODE_BYTES)
-        return filt ? occupancy_of<2, true, true>(smem_block, bps)
-                    : occupancy_of<2, true, false>(smem_block, bps);
-    if (mode == MODE_EXACT) {
-        if (u8) return filt ? occupancy_of<1, true, true>(smem_block, bps)
-                            : occupancy_of<1, true, false>(smem_block, bps);
-        return filt ? occupancy_of<1, false, true>(smem_block, bps)
-                    : occupancy_of<1, false, false>(smem_block, bps);
+template <int MODE, bool U8, int CFG>
+int occupancy_cfg(bool filt, size_t smem_block, int *bps) {
+    return filt ? occupancy_of<MODE, U8, true, CFG>(smem_block, bps)
+                : occupancy_of<MODE, U8, false, CFG>(smem_block, bps);
+}
+
+int occupancy(int mode, bool u8, bool filt, int cfg, size_t smem_block, int *bps) {
+    if (mode == MODE_BYTES) {
+        switch (cfg) {
+            case 1: return occupancy_cfg<2, true, 1>(filt, smem_block, bps);
+            case 2: return occupancy_cfg<2, true, 2>(filt, smem_block, bps);
+            case 3: return occupancy_cfg<2, true, 3>(filt, smem_block, bps);
+            default: return occupancy_cfg<2, true, 0>(filt, smem_block, bps);
+        }
     }
-    if (u8) return filt ? occupancy_of<0, true, true>(smem_block, bps)
-                        : occupancy_of<0, true, false>(smem_block, bps);
-    return filt ? occupancy_of<0, false, true>(smem_block, bps)
-                : occupancy_of<0, false, false>(smem_block, bps);
+    if (mode == MODE_EXACT)
+        return u8 ? occupancy_cfg<1, true, 0>(filt, smem_block, bps)
+                  : occupancy_cfg<1, false, 0>(filt, smem_block, bps);
+    return u8 ? occupancy_cfg<0, true, 0>(filt, smem_block, bps)
+              : occupancy_cfg<0, false, 0>(filt, smem_block, bps);
 }
 
 int ilog2_ceil(int64_t x) {
@@ -1879,7 +1888,19 @@ int hnsw_b200_prof_read(unsigned long long *out, int reset) {
 
 const char *hnsw_b200_last_error(void) { return hb::g_err.c_str(); }
 
-const char *hnsw_b200_version(void) { return "hnsw_b200 0.1 sm_100a"; }
+const char *hnsw_b200_version(void) { return "hnsw_b200 0.2 sm_100a"; }
+
+int32_t hnsw_b200_kernel_configs(int32_t dist_mode) {
+    const int mode = dist_mode == HNSW_B200_DIST_BYTES
+                         ? MODE_BYTES
+                         : (dist_mode == HNSW_B200_DIST_EXACT_F32 ? MODE_EXACT : MODE_F64);
+    return configs_of(mode);
+}
+
+const char *hnsw_b200_kernel_config_name(int32_t dist_mode, int32_t config) {
+    if (config < 0 || config >= hnsw_b200_kernel_configs(dist_mode)) return "";
+    return cfg_name(config);
+}
 
 int hnsw_b200_open(const hnsw_b200_graph_t *graph, void **handle) {
     if (!graph || !handle) return fail(HNSW_B200_EINVAL, "null argument");
@@ -1960,12 +1981,16 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
     const int s_cap = 256;
+    const int cfg = a->kernel_config;
+    if (cfg < 0 || cfg >= configs_of(mode))
+        return fail(HNSW_B200_EINVAL, "kernel_config " + std::to_string(cfg) + " out of range (" +
+                                          std::to_string(configs_of(mode)) + " for this mode)");
     // One lane per neighbour's row: a win unless the filter is very selective, where most rows it
     // would fetch early belong to neighbours already visited.
     const double p = filt ? std::max(double(a->allowed_fraction), 1.0 / double(g.n)) : 1.0;
     const int lane_rows = (!filt || p >= 0.05) ? 1 : 0;
     const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr, g.node_ids != nullptr,
-                                      stage_bytes(mode, lane_rows, g.dim));
+                                      stage_bytes(mode, cfg, lane_rows, g.dim));
     const bool use_mlp = a->stop_mlp != nullptr && !filt;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (a->trace_feat && (!a->trace_dk || !a->trace_count || !a->trace_hops || a->trace_cap < 1))
@@ -1974,7 +1999,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory (" +
                                           std::to_string(smem_block) + " bytes per block)");
     int bps = 0;
-    if (int rc = occupancy(mode, u8, filt, smem_block, &bps)) return rc;
+    if (int rc = occupancy(mode, u8, filt, cfg, smem_block, &bps)) return rc;
     if (bps < 1) return fail(HNSW_B200_EINVAL, "search kernel cannot be resident");
     const int32_t nq = int32_t(a->nq);
 
@@ -2068,8 +2093,8 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     for (int attempt = 0; attempt < 6; attempt++) {
         const int blocks = int(std::min<int64_t>(int64_t(h.sms) * bps, (n_work + WPB - 1) / WPB));
         const int64_t slots = int64_t(blocks) * WPB;
-        // Unfiltered layer 0 uses the bitmap unless built with its hash (HB_L0_HASH).
-        const int64_t vis_stride = int64_t(1) << (HB_L0_HASH && !filt ? std::max(vis_log2, vis_up_log2)
+        // Unfiltered layer 0 uses the bitmap unless the configuration uses its hash.
+        const int64_t vis_stride = int64_t(1) << (cfg_hash(cfg) && !filt ? std::max(vis_log2, vis_up_log2)
                                                                       : vis_up_log2);
         if (int rc = h.vis.ensure(size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
         if (h.bits_dirty && h.vbits.ptr) {
@@ -2102,10 +2127,11 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         P.qlist = qlist;
         P.n_work = n_work;
         CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(int32_t), s));
-        if (int rc = dispatch(h, P, mode, u8, filt, smem_block, blocks, s)) {
+        if (int rc = dispatch(P, mode, u8, filt, cfg, smem_block, blocks, s)) {
             h.bits_dirty = true;
             return rc;
         }
+        h.launches++;
         CUDA_TRY(cudaMemcpyAsync(h.host_pinned, ctr, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         if (cudaStreamSynchronize(s) != cudaSuccess) {
             h.bits_dirty = true;
@@ -2179,6 +2205,8 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     if (a->allowed) return fail(HNSW_B200_EINVAL, "search_noalloc: filtered search needs hnsw_b200_search");
     if (a->priority)
         return fail(HNSW_B200_EINVAL, "search_noalloc: no start order (priority must be NULL)");
+    if (a->kernel_config != 0)
+        return fail(HNSW_B200_EINVAL, "search_noalloc: runs kernel configuration 0 only");
     if (a->nq < 0) return fail(HNSW_B200_EINVAL, "nq out of range");
     if (a->nq > HB_NOALLOC_MAX_NQ)
         return fail(HNSW_B200_EINVAL, "search_noalloc: at most " + std::to_string(HB_NOALLOC_MAX_NQ) +
@@ -2204,7 +2232,7 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     const int ef_cap = std::max(std::max(a->ef_max, a->k_search), 1);
     const int krr = a->rerank_queries ? a->k : 0;
     const size_t wb = warp_smem_bytes(ef_cap, g.dim, false, 256, krr, g.node_ids != nullptr,
-                                      stage_bytes(mode, 1, g.dim));
+                                      stage_bytes(mode, 0, 1, g.dim));
     const bool use_mlp = a->stop_mlp != nullptr;
     const size_t smem_block = wb * WPB + (use_mlp ? al16(MLP_BYTES) : 0);
     if (smem_block > 227 * 1024) return fail(HNSW_B200_EINVAL, "ef/dim too large for shared memory");
@@ -2224,7 +2252,7 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
                                           " nodes needs more than the fixed " +
                                           std::to_string(HB_NOALLOC_BYTES >> 20) + " MiB scratch");
     int bps = 0;
-    if (int rc = occupancy(mode, u8, false, smem_block, &bps)) return rc;
+    if (int rc = occupancy(mode, u8, false, 0, smem_block, &bps)) return rc;
     if (bps < 1) return fail(HNSW_B200_EINVAL, "search kernel cannot be resident");
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -2309,15 +2337,7 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     P.n_cells = a->n_cells;
     P.trace_k = 16;
     P.lane_rows = 1;
-    int rc = 0;
-    if (mode == MODE_BYTES)
-        rc = launch_one_noalloc<MODE_BYTES, true>(P, smem_block, blocks, s);
-    else if (mode == MODE_EXACT)
-        rc = u8 ? launch_one_noalloc<MODE_EXACT, true>(P, smem_block, blocks, s)
-                : launch_one_noalloc<MODE_EXACT, false>(P, smem_block, blocks, s);
-    else
-        rc = u8 ? launch_one_noalloc<MODE_F64, true>(P, smem_block, blocks, s)
-                : launch_one_noalloc<MODE_F64, false>(P, smem_block, blocks, s);
+    const int rc = dispatch(P, mode, u8, false, 0, smem_block, blocks, s);
     if (rc) return rc;
     int32_t failed = 0;  // pageable host copy: no pinned allocation either
     CUDA_TRY(cudaMemcpyAsync(&failed, ctr + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));

@@ -32,6 +32,27 @@ UPLOAD_THREADS = 8
 # DeviceGraph._build_internal_order); smaller ones fit in L2 and keep the reference's order.
 LOCALITY_MIN_NODES = 65536
 LOCALITY_CELLS = 256
+# Autotuner: a configuration replaces the default only when it is this much faster.
+TUNE_MARGIN = 0.02
+TUNE_REPS = 3
+
+
+def pick_config(ms: list[float], default: int = 0, margin: float = TUNE_MARGIN) -> int:
+    """The kernel configuration to keep from measured times (one per configuration, same batch):
+    the fastest, if it beats the default by more than ``margin``, else the default. A function of
+    the timings alone, so the same measurements always give the same choice."""
+    if not ms:
+        return default
+    best = min(range(len(ms)), key=lambda c: (ms[c], c))
+    return best if ms[best] < (1.0 - margin) * ms[default] else default
+
+
+def tune_key(dist_mode: int, use_codes: bool, filtered: bool, ef_cap: int, stop: bool,
+             rerank: bool) -> tuple:
+    """What a tuned choice is kept for: the kernel (distance mode, rows, filter), the learned stop
+    and the rerank epilogue, and the efSearch cap rounded up to a power of two."""
+    bucket = 1 << max(0, int(ef_cap) - 1).bit_length()
+    return (int(dist_mode), bool(use_codes), bool(filtered), bucket, bool(stop), bool(rerank))
 
 
 def _dev_ptr(t: torch.Tensor | None) -> int | None:
@@ -137,6 +158,11 @@ class DeviceGraph:
         self._stage: torch.Tensor | None = None
         self._stage_done = torch.cuda.Event()
         self._internal: dict[str, Any] = {}
+        # Runtime autotuner (see search): kernel configuration per tune_key, with the timings that
+        # chose it.
+        self.autotune = True
+        self.tuned: dict[tuple, int] = {}
+        self.tune_log: dict[tuple, list[float]] = {}
         if validate_M is not None:  # before anything follows the links
             self._validate_on_device(arrays["levels"], int(validate_M))
         if self.locality:
@@ -481,6 +507,7 @@ class DeviceGraph:
         out: tuple[torch.Tensor, ...] | None = None,
         stop: tuple[torch.Tensor, float] | None = None,
         trace: tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor] | None = None,
+        kernel_config: int | None = None,
     ) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor | None]:
         """One batched search; returns device tensors ``(ids, dists, counters)``.
 
@@ -498,6 +525,12 @@ class DeviceGraph:
         Batches of at least ``schedule.MIN_QUERIES`` on graphs of at least ``LOCALITY_MIN_NODES``
         nodes start longest-predicted first (``self.schedule``; see :mod:`.schedule`); results
         do not depend on it.
+
+        ``kernel_config``: the kernel configuration (``hnsw_b200_kernel_configs``); by default the
+        autotuner's choice for this kind of batch. With ``self.autotune`` the first batch of at
+        least ``schedule.MIN_QUERIES`` queries of each kind (:func:`tune_key`) is searched once
+        per configuration, ``TUNE_REPS`` times each, timed with CUDA events, and the choice of
+        :func:`pick_config` is kept for later batches. Results do not depend on the configuration.
         """
         dev = self.device
         nq = int(queries.shape[0])
@@ -580,6 +613,35 @@ class DeviceGraph:
                 cell_cost=_dev_ptr(sched.cost) if learn else None,
                 n_cells=sched.n_cells if learn else 0,
             )
-            stream = torch.cuda.current_stream(dev).cuda_stream
-            _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args), ctypes.c_void_p(stream)))
+            stream = torch.cuda.current_stream(dev)
+            key = tune_key(dist_mode, use_codes, bitmap is not None, max(ef_max, ks), stop is not None,
+                           rq is not None)
+            if kernel_config is None:
+                n_cfg = int(self.lib.hnsw_b200_kernel_configs(int(dist_mode)))
+                if (self.autotune and key not in self.tuned and n_cfg > 1 and nq >= MIN_QUERIES
+                        and trace is None):
+                    self._tune(args, key, n_cfg, stream)
+                kernel_config = self.tuned.get(key, 0)
+            args.kernel_config = int(kernel_config)
+            _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args),
+                                                 ctypes.c_void_p(stream.cuda_stream)))
         return ids, dists, ctr
+
+    def _tune(self, args: _lib.SearchArgs, key: tuple, n_cfg: int, stream: torch.cuda.Stream) -> None:
+        """Time every kernel configuration on this batch (median of ``TUNE_REPS`` launches each)
+        and keep :func:`pick_config`'s choice for ``key``."""
+        ms = []
+        for cfg in range(n_cfg):
+            args.kernel_config = cfg
+            times = []
+            for _ in range(TUNE_REPS):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args),
+                                                     ctypes.c_void_p(stream.cuda_stream)))
+                b.record(stream)
+                b.synchronize()
+                times.append(a.elapsed_time(b))
+            ms.append(float(np.median(times)))
+        self.tuned[key] = pick_config(ms)
+        self.tune_log[key] = ms

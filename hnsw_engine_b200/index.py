@@ -330,7 +330,7 @@ class HNSWIndex:
         if not flags[0]:
             raise ValueError("vectors contains NaN or infinite values")
         if flags[1]:
-            rows_host = torch.flatnonzero(norms[:, 0] == 0)[:5].cpu().tolist()
+            rows_host = torch.nonzero(norms[:, 0] == 0).flatten()[:5].cpu().tolist()
             raise ValueError(f"cosine distance is undefined for zero vectors (rows {rows_host})")
         if not flags[2]:
             raise ValueError("vectors overflow float32 (values beyond about 3.4e38)")

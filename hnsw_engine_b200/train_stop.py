@@ -127,13 +127,17 @@ def main() -> None:
     p.add_argument("--n-train", type=int, default=200_000)
     p.add_argument("--ef-cap", type=int, default=192)
     p.add_argument("--epochs", type=int, default=4)
+    p.add_argument("--target", type=float, default=0.95,
+                   help="recall@10 target of the threshold (a graph that cannot reach 0.95 at "
+                        "the cap efSearch is tuned to what it can reach)")
     p.add_argument("--retune", action="store_true",
                    help="only re-tune the shipped network's threshold for the current schedule")
     args = p.parse_args()
     if args.retune:
         print(json.dumps(retune(args.workload)), flush=True)
         return
-    print(json.dumps(train(args.workload, args.n_train, args.ef_cap, epochs=args.epochs)), flush=True)
+    print(json.dumps(train(args.workload, args.n_train, args.ef_cap, target=args.target,
+                           epochs=args.epochs)), flush=True)
 
 
 if __name__ == "__main__":

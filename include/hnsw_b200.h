@@ -130,6 +130,9 @@ typedef struct hnsw_b200_search_args {
     const int32_t *cells;
     double *cell_cost;
     int32_t n_cells;
+    /* Kernel configuration, 0 .. hnsw_b200_kernel_configs(dist_mode) - 1 (0: the default). Every
+     * configuration returns the same results; they differ in speed (the autotuner's choices). */
+    int32_t kernel_config;
 } hnsw_b200_search_args_t;
 
 #define HNSW_B200_STOP_EVERY 16
@@ -225,6 +228,14 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *args, void *st
  *   - it waits for `stream` once, to read the overflow count into host memory, before returning. */
 int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph, const hnsw_b200_search_args_t *args,
                              void *stream);
+
+/* Kernel configurations of the search for a distance mode (no reference counterpart: the
+ * autotuner's choices). The byte kernels have four: the layer-0 visited set as a per-slot bitmap or
+ * an open-addressing hash, gathered rows held in registers or staged in shared memory by cp.async,
+ * and 5 or 4 resident blocks per SM (the register cap); the other modes have one. The name is a
+ * static string ("" for an index out of range). */
+int32_t hnsw_b200_kernel_configs(int32_t dist_mode);
+const char *hnsw_b200_kernel_config_name(int32_t dist_mode, int32_t config);
 
 /* Number of device kernel launches made by the last hnsw_b200_search on this handle. */
 int64_t hnsw_b200_last_launches(void *handle);
