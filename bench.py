@@ -488,7 +488,10 @@ def main() -> None:
         pg.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
+        # NVTX range "timed_learned": lets a profiler list exactly the value's launches
+        torch.cuda.nvtx.range_push("timed_learned")
         ms_learned = timed_steps(step_learned, args.steps, stream)
+        torch.cuda.nvtx.range_pop()
         ms_fine = timed_steps(step_fine, args.steps, stream)
         ms_plain = timed_steps(step_plain, args.steps, stream)
         ms_in = timed_steps(step_in_sample, max(3, args.steps // 4), stream)

@@ -156,6 +156,10 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
                                                 ctypes.c_void_p, ctypes.c_void_p]),
     "hnsw_b200_version": (ctypes.c_char_p, []),
     "hnsw_b200_kernel_configs": (ctypes.c_int32, [ctypes.c_int32]),
+    "hnsw_b200_search_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchArgs),
+                                              ctypes.c_void_p]),
+    "hnsw_b200_search_failed": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                               ctypes.c_void_p]),
     "hnsw_b200_kernel_config_name": (ctypes.c_char_p, [ctypes.c_int32, ctypes.c_int32]),
 }
 

@@ -84,6 +84,15 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_ADMIT_MASKS
 #define HB_ADMIT_MASKS 1
 #endif
+// Batched admission: rank each new neighbour in the results by a 4-ary search (three independent
+// shared-memory reads per step) instead of a binary search.
+#ifndef HB_KARY_SEARCH
+#define HB_KARY_SEARCH 0
+#endif
+// Pop of the next unexpanded result: one shared-memory round instead of three.
+#ifndef HB_FAST_POP
+#define HB_FAST_POP 0
+#endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
 #define HB_PROF_DECL unsigned long long hb_t = clock64();
@@ -1018,12 +1027,45 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
     const bool inc = (cm >> lane) & 1u;
     int lo = 0, n_eq = 0, eq_lt = 0;
     if (inc) {
+#if HB_KARY_SEARCH
+        // lo: entries of R0 with distance below dj. The answer stays in [a, a + len]; each step
+        // reads three independent split points (one round trip to shared memory) and keeps one
+        // quarter, then a binary search finishes.
+        int a = 0, len = r0;
+        while (len >= 4) {
+            const int q = len >> 2;
+            const int s1 = a + q, s2 = a + 2 * q, s3 = a + 3 * q;
+            const bool b1 = C.Rd[s1] < dj, b2 = C.Rd[s2] < dj, b3 = C.Rd[s3] < dj;
+            if (b3) {
+                len = a + len - s3 - 1;
+                a = s3 + 1;
+            } else if (b2) {
+                a = s2 + 1;
+                len = q - 1;
+            } else if (b1) {
+                a = s1 + 1;
+                len = q - 1;
+            } else {
+                len = q;
+            }
+        }
+        while (len > 0) {
+            const int m = a + (len >> 1);
+            if (C.Rd[m] < dj) {
+                a = m + 1;
+                len = len - (len >> 1) - 1;
+            } else {
+                len >>= 1;
+            }
+        }
+#else
         int a = 0, b = r0;  // lo: entries of R0 with distance below dj
         while (a < b) {
             const int m = (a + b) >> 1;
             if (C.Rd[m] < dj) a = m + 1;
             else b = m;
         }
+#endif
         lo = a;
         for (int i = a; i < r0 && C.Rd[i] == dj; i++) {  // equal distances: rank by id
             n_eq++;
@@ -1173,6 +1215,22 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
         int32_t c = -1;
         while (scan < r) {
             const int i = scan + lane;
+#if HB_FAST_POP
+            // Every lane reads its entry's two ids at once; the first unexpanded lane marks its
+            // entry expanded and its internal id comes by shuffle (the ballot orders these writes
+            // after every lane's read).
+            const int32_t ri = i < r ? C.Ri[i] : EXP_BIT;
+            const int32_t rp = i < r ? C.Rp[i] : 0;
+            const uint32_t b = __ballot_sync(FULL, !(ri & EXP_BIT));
+            if (b) {
+                const int j = __ffs(b) - 1;
+                if (lane == j) C.Ri[i] = ri | EXP_BIT;
+                c = __shfl_sync(FULL, rp, j) & ID_MASK;
+                scan += j + 1;
+                __syncwarp();
+                break;
+            }
+#else
             const bool un = i < r && !(C.Ri[i] & EXP_BIT);
             const uint32_t b = __ballot_sync(FULL, un);
             if (b) {
@@ -1185,6 +1243,7 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
                 __syncwarp();
                 break;
             }
+#endif
             scan += 32;
         }
         if (c < 0) {
@@ -1953,13 +2012,19 @@ int64_t hnsw_b200_last_launches(void *handle) {
     return handle ? static_cast<Handle *>(handle)->launches : 0;
 }
 
-int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *stream) {
-    if (!handle || !a) return fail(HNSW_B200_EINVAL, "null argument");
-    Handle &h = *static_cast<Handle *>(handle);
-    std::lock_guard<std::mutex> lock(h.mu);
+}  // extern "C"
+
+namespace hb {
+
+// The batched search. async = false: allocate scratch as needed, wait for the stream to read the
+// overflow count and re-run overflowed queries with larger scratch. async = true: allocate nothing,
+// synchronise nothing and read nothing on the host -- every launch goes on the stream (so a stream
+// capture can record them); the scratch must already fit (a synchronous call with arguments of
+// the same size sized it), and overflowed queries stay unwritten with their count left on the
+// device for hnsw_b200_search_failed.
+int search_impl(Handle &h, const hnsw_b200_search_args_t *a, cudaStream_t s, bool async) {
     h.launches = 0;
     const hnsw_b200_graph_t &g = h.g;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (a->nq < 0 || a->nq > 0x7fffffff) return fail(HNSW_B200_EINVAL, "nq out of range");
     if (a->nq == 0) return 0;
     if (a->k < 1 || a->k_search < a->k) return fail(HNSW_B200_EINVAL, "need 1 <= k <= k_search");
@@ -2013,10 +2078,20 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
     const int vlist_cap = int(std::min<int64_t>(65536, std::max<int64_t>(256, g.n / 256)));
     int spill_cap = filt ? int(std::min(double(g.n) + 64.0, est)) : 0;
 
-    if (int rc = h.counters.ensure(4 * sizeof(int32_t))) return rc;
-    if (int rc = h.status.ensure(size_t(nq) * sizeof(int32_t))) return rc;
-    if (int rc = h.qlist[0].ensure(size_t(nq) * sizeof(int32_t))) return rc;
-    if (int rc = h.qlist[1].ensure(size_t(nq) * sizeof(int32_t))) return rc;
+    // Scratch: grown (zero-filled where noted) by a synchronous call; an asynchronous call only
+    // checks that what it needs is already there.
+    auto need = [&](Buffer &b, size_t bytes, bool zero = false) -> int {
+        if (!async) return b.ensure(bytes, zero, s);
+        if (b.bytes >= bytes && b.ptr) return 0;
+        return fail(HNSW_B200_EINVAL, "search_async: scratch for this batch is not reserved (run "
+                                      "hnsw_b200_search once with arguments of this size first)");
+    };
+    if (int rc = need(h.counters, 4 * sizeof(int32_t))) return rc;
+    if (int rc = need(h.status, size_t(nq) * sizeof(int32_t))) return rc;
+    if (!async) {
+        if (int rc = h.qlist[0].ensure(size_t(nq) * sizeof(int32_t))) return rc;
+        if (int rc = h.qlist[1].ensure(size_t(nq) * sizeof(int32_t))) return rc;
+    }
     int32_t *ctr = static_cast<int32_t *>(h.counters.ptr);
 
     SearchParams P;
@@ -2073,9 +2148,9 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         // First work list: rows by descending priority, stably (CUB radix sort of the low 16 bits
         // of the keys with the rows as values); always a permutation of the rows.
         const size_t rb = size_t(nq) * sizeof(int32_t);
-        if (int rc = h.order_rows.ensure(rb)) return rc;
-        if (int rc = h.order_keys.ensure(rb)) return rc;
-        if (int rc = h.order_list.ensure(rb)) return rc;
+        if (int rc = need(h.order_rows, rb)) return rc;
+        if (int rc = need(h.order_keys, rb)) return rc;
+        if (int rc = need(h.order_list, rb)) return rc;
         int32_t *rows = static_cast<int32_t *>(h.order_rows.ptr);
         int32_t *keys = static_cast<int32_t *>(h.order_keys.ptr);
         int32_t *list = static_cast<int32_t *>(h.order_list.ptr);
@@ -2085,7 +2160,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         size_t temp = 0;
         CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, temp, a->priority, keys, rows,
                                                            list, nq, 0, 16, s));
-        if (int rc = h.sort_temp.ensure(std::max<size_t>(temp, 16))) return rc;
+        if (int rc = need(h.sort_temp, std::max<size_t>(temp, 16))) return rc;
         CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(h.sort_temp.ptr, temp, a->priority, keys,
                                                            rows, list, nq, 0, 16, s));
         qlist = list;
@@ -2096,19 +2171,21 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         // Unfiltered layer 0 uses the bitmap unless the configuration uses its hash.
         const int64_t vis_stride = int64_t(1) << (cfg_hash(cfg) && !filt ? std::max(vis_log2, vis_up_log2)
                                                                       : vis_up_log2);
-        if (int rc = h.vis.ensure(size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
+        if (int rc = need(h.vis, size_t(slots * vis_stride) * sizeof(int32_t))) return rc;
         if (h.bits_dirty && h.vbits.ptr) {
+            if (async) return fail(HNSW_B200_EINVAL, "search_async: a failed launch left the bitmaps "
+                                                     "dirty; run hnsw_b200_search first");
             CUDA_TRY(cudaMemsetAsync(h.vbits.ptr, 0, h.vbits.bytes, s));
             h.bits_dirty = false;
         }
-        if (int rc = h.vbits.ensure(size_t(slots * vbits_stride) * sizeof(uint32_t), true, s)) return rc;
-        if (int rc = h.vlist.ensure(size_t(slots) * vlist_cap * sizeof(int32_t))) return rc;
-        if (int rc = h.ties.ensure(size_t(slots) * tie_cap * sizeof(int32_t))) return rc;
+        if (int rc = need(h.vbits, size_t(slots * vbits_stride) * sizeof(uint32_t), true)) return rc;
+        if (int rc = need(h.vlist, size_t(slots) * vlist_cap * sizeof(int32_t))) return rc;
+        if (int rc = need(h.ties, size_t(slots) * tie_cap * sizeof(int32_t))) return rc;
         if (filt) {
-            if (int rc = h.spill_d.ensure(size_t(slots) * spill_cap * sizeof(double))) return rc;
-            if (int rc = h.spill_i.ensure(size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
+            if (int rc = need(h.spill_d, size_t(slots) * spill_cap * sizeof(double))) return rc;
+            if (int rc = need(h.spill_i, size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
             if (g.node_ids)
-                if (int rc = h.spill_p.ensure(size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
+                if (int rc = need(h.spill_p, size_t(slots) * spill_cap * sizeof(int32_t))) return rc;
         }
         P.vbits = static_cast<uint32_t *>(h.vbits.ptr);
         P.vbits_stride = vbits_stride;
@@ -2132,6 +2209,7 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
             return rc;
         }
         h.launches++;
+        if (async) return 0;  // the overflow count stays on the device
         CUDA_TRY(cudaMemcpyAsync(h.host_pinned, ctr, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         if (cudaStreamSynchronize(s) != cudaSuccess) {
             h.bits_dirty = true;
@@ -2158,6 +2236,40 @@ int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *strea
         if (filt) spill_cap = int(std::min<int64_t>(int64_t(spill_cap) * 4, g.n + 64));
     }
     return fail(HNSW_B200_ERETRY, "queries still overflowed scratch after retries");
+}
+
+}  // namespace hb
+
+extern "C" {
+
+int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *a, void *stream) {
+    if (!handle || !a) return fail(HNSW_B200_EINVAL, "null argument");
+    Handle &h = *static_cast<Handle *>(handle);
+    std::lock_guard<std::mutex> lock(h.mu);
+    return search_impl(h, a, static_cast<cudaStream_t>(stream), false);
+}
+
+int hnsw_b200_search_async(void *handle, const hnsw_b200_search_args_t *a, void *stream) {
+    if (!handle || !a) return fail(HNSW_B200_EINVAL, "null argument");
+    Handle &h = *static_cast<Handle *>(handle);
+    std::lock_guard<std::mutex> lock(h.mu);
+    return search_impl(h, a, static_cast<cudaStream_t>(stream), true);
+}
+
+int hnsw_b200_search_failed(void *handle, int32_t *failed, void *stream) {
+    if (!handle || !failed) return fail(HNSW_B200_EINVAL, "null argument");
+    Handle &h = *static_cast<Handle *>(handle);
+    std::lock_guard<std::mutex> lock(h.mu);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!h.counters.ptr) {
+        *failed = 0;
+        return 0;
+    }
+    CUDA_TRY(cudaMemcpyAsync(h.host_pinned, static_cast<int32_t *>(h.counters.ptr),
+                             4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    *failed = h.host_pinned[1];
+    return 0;
 }
 
 }  // extern "C"

@@ -90,6 +90,52 @@ def to_device(a: Any, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
     return t.to(device, non_blocking=False).contiguous()
 
 
+class CapturedSearch:
+    """One batched search recorded as a CUDA graph and replayed: the start-order launches, the
+    counters' reset and the search kernel, with no host work between them.
+
+    The queries live in a fixed device buffer (``self.queries``): copy each new batch into it,
+    then :meth:`replay`. Construction runs the search once synchronously with the same arguments,
+    which sizes the scratch, picks the distance arithmetic from the buffer's current contents and
+    lets the autotuner choose the kernel configuration; the graph keeps those choices, so later
+    batches must suit the same arithmetic (byte mode: integer queries in [0, 255]).
+    :meth:`results` returns the outputs after checking on the host that no query overflowed its
+    scratch, re-running the batch synchronously in that rare case."""
+
+    def __init__(self, graph: "DeviceGraph", queries: torch.Tensor, k: int, ef: int, *,
+                 stop: tuple | None = None) -> None:
+        self.graph = graph
+        self.queries = queries.to(device=graph.device, dtype=torch.float32).contiguous()
+        self.k, self.ef, self.stop = int(k), int(ef), stop
+        nq = self.queries.shape[0]
+        dev = graph.device
+        with torch.cuda.device(dev):
+            self.out = (torch.empty((nq, k), dtype=torch.int64, device=dev),
+                        torch.empty((nq, k), dtype=torch.float64, device=dev),
+                        torch.empty((nq, 2), dtype=torch.int64, device=dev))
+            graph.search(self.queries, k, ef, stop=stop, out=self.out)
+            self.dist_mode = graph.last_call["dist_mode"]
+            self.kernel_config = graph.last_call["kernel_config"]
+            torch.cuda.synchronize(dev)
+            self.cuda_graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.cuda_graph):
+                graph.search(self.queries, k, ef, stop=stop, out=self.out, dist_mode=self.dist_mode,
+                             kernel_config=self.kernel_config, asynchronous=True)
+            graph._priority_launches = 0
+
+    def replay(self) -> None:
+        """Run the recorded search on the buffer's current queries (asynchronous)."""
+        self.cuda_graph.replay()
+
+    def results(self) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """(ids, distances, counters) of the last replay; overflowed queries (none in practice)
+        are searched again synchronously."""
+        if self.graph.search_failed():
+            self.graph.search(self.queries, self.k, self.ef, stop=self.stop, out=self.out,
+                              dist_mode=self.dist_mode, kernel_config=self.kernel_config)
+        return self.out
+
+
 class DeviceGraph:
     """A reference-built HNSW graph resident on one GPU, plus its library handle."""
 
@@ -161,6 +207,7 @@ class DeviceGraph:
         # Runtime autotuner (see search): kernel configuration per tune_key, with the timings that
         # chose it.
         self.autotune = True
+        self.last_call: dict[str, int] = {}  # dist_mode and kernel_config of the last search
         self.tuned: dict[tuple, int] = {}
         self.tune_log: dict[tuple, list[float]] = {}
         if validate_M is not None:  # before anything follows the links
@@ -508,6 +555,8 @@ class DeviceGraph:
         stop: tuple[torch.Tensor, float] | None = None,
         trace: tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor] | None = None,
         kernel_config: int | None = None,
+        asynchronous: bool = False,
+        ef_max: int | None = None,
     ) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor | None]:
         """One batched search; returns device tensors ``(ids, dists, counters)``.
 
@@ -531,6 +580,13 @@ class DeviceGraph:
         least ``schedule.MIN_QUERIES`` queries of each kind (:func:`tune_key`) is searched once
         per configuration, ``TUNE_REPS`` times each, timed with CUDA events, and the choice of
         :func:`pick_config` is kept for later batches. Results do not depend on the configuration.
+
+        ``asynchronous``: issue the search with no host synchronisation, allocation or read-back
+        (``hnsw_b200_search_async``), so that it can be recorded in a CUDA graph
+        (:class:`CapturedSearch`). It needs ``dist_mode`` and ``kernel_config`` given, a
+        device float tensor of queries, ``ef`` an int or a device tensor with ``ef_max``, no host
+        filter mask, and scratch sized by an earlier synchronous call of the same size.
+        Overflowed queries are left unwritten; :meth:`search_failed` counts them.
         """
         dev = self.device
         nq = int(queries.shape[0])
@@ -538,11 +594,16 @@ class DeviceGraph:
         q_f64 = use_codes
         with torch.cuda.device(dev):
             q = to_device(queries, torch.float64 if q_f64 else torch.float32, dev)
+            if asynchronous and (dist_mode is None or kernel_config is None):
+                raise ValueError("an asynchronous search needs dist_mode and kernel_config")
             if dist_mode is None:
                 dist_mode = self.choose_mode_device(q, use_codes)
             if isinstance(ef, torch.Tensor):
                 ef_t = ef.to(device=dev, dtype=torch.int32).contiguous()
-                ef_max = int(ef_t.max().item()) if nq else 1
+                if ef_max is None:
+                    if asynchronous:
+                        raise ValueError("an asynchronous search with per-query ef needs ef_max")
+                    ef_max = int(ef_t.max().item()) if nq else 1
             elif np.ndim(ef) == 0:
                 ef_max = int(ef) if nq else 1
                 ef_t = torch.full((nq,), int(ef), dtype=torch.int32, device=dev)
@@ -623,9 +684,20 @@ class DeviceGraph:
                     self._tune(args, key, n_cfg, stream)
                 kernel_config = self.tuned.get(key, 0)
             args.kernel_config = int(kernel_config)
-            _lib.check(self.lib.hnsw_b200_search(self._handle, ctypes.byref(args),
-                                                 ctypes.c_void_p(stream.cuda_stream)))
+            self.last_call = {"dist_mode": int(dist_mode), "kernel_config": int(kernel_config)}
+            fn = self.lib.hnsw_b200_search_async if asynchronous else self.lib.hnsw_b200_search
+            _lib.check(fn(self._handle, ctypes.byref(args), ctypes.c_void_p(stream.cuda_stream)))
         return ids, dists, ctr
+
+    def search_failed(self) -> int:
+        """Queries the last asynchronous search left unwritten (their scratch overflowed); waits
+        for the current stream."""
+        out = ctypes.c_int32(0)
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(self.lib.hnsw_b200_search_failed(self._handle, ctypes.byref(out),
+                                                        ctypes.c_void_p(stream)))
+        return int(out.value)
 
     def _tune(self, args: _lib.SearchArgs, key: tuple, n_cfg: int, stream: torch.cuda.Stream) -> None:
         """Time every kernel configuration on this batch (median of ``TUNE_REPS`` launches each)

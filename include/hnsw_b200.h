@@ -205,6 +205,18 @@ void hnsw_b200_close(void *handle);
  * larger scratch; results are complete when it returns 0. */
 int hnsw_b200_search(void *handle, const hnsw_b200_search_args_t *args, void *stream);
 
+/* The same search as hnsw_b200_search, issued with no host synchronisation, no allocation and
+ * no host read, every launch on `stream`, so that it can be recorded in a CUDA graph and replayed
+ * (the reference's search has no counterpart: it runs on the CPU). The handle's scratch must
+ * already fit the arguments: a hnsw_b200_search call with arguments of the same size (queries,
+ * ef_max, k, filter, rerank, kernel configuration) sizes it, else HNSW_B200_EINVAL. Queries that
+ * overflow their scratch are left unwritten and counted on the device: read the count with
+ * hnsw_b200_search_failed once the stream has run the search, and search them again with
+ * hnsw_b200_search. */
+int hnsw_b200_search_async(void *handle, const hnsw_b200_search_args_t *args, void *stream);
+/* Queries the last hnsw_b200_search_async on this handle left unwritten; synchronises `stream`. */
+int hnsw_b200_search_failed(void *handle, int32_t *failed, void *stream);
+
 /* Batched search without any device allocation, for callers that are not allowed to allocate
  * GPU memory: real-time serving loops where an allocation would stall the loop, plugins whose host
  * owns every device allocation through its own pool, processes under a hard device-memory budget.
