@@ -701,8 +701,11 @@ class DeviceGraph:
 
     def _tune(self, args: _lib.SearchArgs, key: tuple, n_cfg: int, stream: torch.cuda.Stream) -> None:
         """Time every kernel configuration on this batch (median of ``TUNE_REPS`` launches each)
-        and keep :func:`pick_config`'s choice for ``key``."""
+        and keep :func:`pick_config`'s choice for ``key``. The timing runs do not learn into the
+        start order's cost table (the search that follows does, once)."""
         ms = []
+        learn = (args.cells, args.cell_cost, args.n_cells)
+        args.cells, args.cell_cost, args.n_cells = None, None, 0
         for cfg in range(n_cfg):
             args.kernel_config = cfg
             times = []
@@ -715,5 +718,6 @@ class DeviceGraph:
                 b.synchronize()
                 times.append(a.elapsed_time(b))
             ms.append(float(np.median(times)))
+        args.cells, args.cell_cost, args.n_cells = learn
         self.tuned[key] = pick_config(ms)
         self.tune_log[key] = ms

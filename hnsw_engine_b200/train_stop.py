@@ -13,7 +13,8 @@
 
     python -m hnsw_engine_b200.train_stop --workload mix1m --retune
 
-re-tunes the threshold of the stored network for the current schedule without retraining.
+re-tunes the threshold of the stored network (with its stored threshold schedule) without
+retraining.
 
 The model is written to ``graphs/<workload>/stopnet/`` (git-ignored, next to the graph).
 """
@@ -50,7 +51,8 @@ def _validation(workload: str, index: HNSWIndex, metric: str, k: int, n_val: int
 
 
 def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
-          target: float = 0.95, epochs: int = 4, n_val: int = 10_000, device: str = "cuda") -> dict:
+          target: float = 0.95, epochs: int = 4, n_val: int = 10_000, device: str = "cuda",
+          slope: float = STOP_SLOPE, slope_from: int = STOP_SLOPE_FROM) -> dict:
     t0 = time.time()
     meta, arrays = graphs.open_workload(workload)
     params = {kk: v for kk, v in meta["params"].items() if kk != "engine"}
@@ -72,7 +74,7 @@ def train(workload: str, n_train: int = 200_000, ef_cap: int = 192, k: int = 10,
 
     net = StopNetwork(g.device)
     net.ef_cap = ef_cap
-    net.slope, net.slope_from = STOP_SLOPE, STOP_SLOPE_FROM
+    net.slope, net.slope_from = slope, slope_from
     losses = net.fit(X, y, epochs=epochs)
     log["epoch_losses"] = losses
 
@@ -105,7 +107,7 @@ def load_or_train(workload: str, device: str = "cuda") -> StopNetwork:
 
 def retune(workload: str, path: Path | None = None, k: int = 10, target: float = 0.95,
            n_val: int = 10_000, device: str = "cuda") -> dict:
-    """Re-tune the stored network's threshold for the current schedule on the validation queries
+    """Re-tune the stored network's threshold (its schedule unchanged) on the validation queries
     and write it back (to ``path``, default the shipped copy)."""
     path = SHIPPED / workload if path is None else Path(path)
     net = StopNetwork.load(path, device)
@@ -114,7 +116,6 @@ def retune(workload: str, path: Path | None = None, k: int = 10, target: float =
     index = HNSWIndex.from_arrays(arrays, int(meta["entry_point"]), int(meta["max_level"]),
                                   device=device, **params)
     q_val, val_d = _validation(workload, index, params["metric"], k, n_val)
-    net.slope, net.slope_from = STOP_SLOPE, STOP_SLOPE_FROM
     thr, rec = tune_threshold(index.device_graph, net, q_val, val_d, k, net.ef_cap, target)
     net.save(path)
     return {"workload": workload, "threshold": thr, "slope": net.slope,
@@ -127,6 +128,9 @@ def main() -> None:
     p.add_argument("--n-train", type=int, default=200_000)
     p.add_argument("--ef-cap", type=int, default=192)
     p.add_argument("--epochs", type=int, default=4)
+    p.add_argument("--slope", type=float, default=STOP_SLOPE,
+                   help="threshold rise per 64 layer-0 expansions beyond --slope-from (0: constant)")
+    p.add_argument("--slope-from", type=int, default=STOP_SLOPE_FROM)
     p.add_argument("--target", type=float, default=0.95,
                    help="recall@10 target of the threshold (a graph that cannot reach 0.95 at "
                         "the cap efSearch is tuned to what it can reach)")
@@ -137,7 +141,8 @@ def main() -> None:
         print(json.dumps(retune(args.workload)), flush=True)
         return
     print(json.dumps(train(args.workload, args.n_train, args.ef_cap, target=args.target,
-                           epochs=args.epochs)), flush=True)
+                           epochs=args.epochs, slope=args.slope, slope_from=args.slope_from)),
+          flush=True)
 
 
 if __name__ == "__main__":
