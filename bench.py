@@ -524,6 +524,16 @@ def main() -> None:
     e2e_value = job_throughput(world, nq, 1, e2e_ms)
     assert np.array_equal(e_ids, ids_o.cpu().numpy()), "e2e results differ from device results"
 
+    # The same learned-stop step recorded once as a CUDA graph and replayed.
+    from hnsw_engine_b200.engine import CapturedSearch
+
+    captured = CapturedSearch(g, q_dev, k, cap, stop=(packed, thr, net.slope, net.slope_from))
+    for _ in range(3):
+        captured.replay()
+    ms_graph = timed_steps(captured.replay, args.steps, stream)
+    graph_same = bool(torch.equal(captured.results()[0], ids_o))
+    graph_ms = max_over_ranks(pg, float(np.median(ms_graph)), dev)
+
     # The per-batch audit (2% of each batch against the exact k-NN; plain fixed ef on a miss),
     # over ten batches of a tenth of the queries.
     audits = []
@@ -606,6 +616,8 @@ def main() -> None:
                                 else "row order"),
                 "per_query_ef_32_512": {"qps": job_throughput(world, nq, 1, pq_mean), "recall_at_10": pq_rec,
                                         "achieved_gbs": pq_bytes / (pq_mean / 1000.0) / 1e9},
+                "cuda_graph_replay": {"ms": graph_ms, "qps": job_throughput(world, nq, 1, graph_ms),
+                                      "same_results_as_value": graph_same},
                 "configs": more,
                 "autotune": autotune_report(g),
             },

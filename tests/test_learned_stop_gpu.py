@@ -125,8 +125,11 @@ def test_in_kernel_inference_stops_where_the_network_says(slope: float, slope_fr
 
 
 def test_trained_network_beats_fixed_ef_at_equal_recall() -> None:
-    """On the same held-out queries and recall target, the learned stop computes fewer distances
-    than the smallest fixed efSearch that reaches the target."""
+    """Held out: the network is trained on one set of queries (seed 2), its threshold and the plain
+    arm's efSearch are both fixed on validation queries (seed 9), and both arms are scored and
+    timed on queries neither saw (seed 1). The learned stop computes fewer distances than the
+    plain operating point at the recall target, and its time stays within 10% of plain's (the
+    network's checkpoints cost time; on this data its stops save about as much as they cost)."""
     import torch
 
     from hnsw_engine_b200 import graphs
@@ -137,6 +140,7 @@ def test_trained_network_beats_fixed_ef_at_equal_recall() -> None:
     g, name = _graph()
     k, cap, target = 10, 256, 0.95
     q_tr = graphs.workload_queries(name, nq=20000, seed=2)
+    q_val = graphs.workload_queries(name, nq=2000, seed=9)
     q_ev = graphs.workload_queries(name, nq=2000, seed=1)
     tr = collect_traces(g, q_tr, k, cap)
     _, td = exact_search(g.vectors, torch.from_numpy(q_tr).cuda(), k, "l2")
@@ -144,17 +148,43 @@ def test_trained_network_beats_fixed_ef_at_equal_recall() -> None:
     assert np.isfinite(y).all() and (y >= 0).all()
     net = StopNetwork("cuda")
     net.fit(X, y, epochs=4)
-    _, ev_d = exact_search(g.vectors, torch.from_numpy(q_ev).cuda(), k, "l2")
-    ev_d = ev_d.cpu().numpy()
-    thr, rec = tune_threshold(g, net, q_ev, ev_d, k, cap, target)
-    assert rec >= target
-    ids, d, ctr = g.search(q_ev, k, cap, stop=(net.packed(), thr))
-    learned_dists = int(ctr[:, 0].sum())
-    plain = None
+
+    def gt(q):
+        return exact_search(g.vectors, torch.from_numpy(q).cuda(), k, "l2")[1].cpu().numpy()
+
+    val_d, ev_d = gt(q_val), gt(q_ev)
+    thr, rec_val = tune_threshold(g, net, q_val, val_d, k, cap, target)
+    assert rec_val >= target
+    ef_op = None
     for ef in (10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256):
-        ids, d, ctr = g.search(q_ev, k, ef)
-        if recall_of(ids.cpu().numpy(), d.cpu().numpy(), ev_d, k) >= target:
-            plain = int(ctr[:, 0].sum())
+        ids, d, _ = g.search(q_val, k, ef)
+        if recall_of(ids.cpu().numpy(), d.cpu().numpy(), val_d, k) >= target:
+            ef_op = ef
             break
-    assert plain is not None
-    assert learned_dists < plain, (learned_dists, plain)
+    assert ef_op is not None
+    qd = torch.from_numpy(q_ev).cuda()
+    packed = net.packed()
+
+    def run(stop):
+        kw = {"stop": (packed, thr)} if stop else {}
+        out = g.search(qd, k, cap if stop else ef_op, **kw)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            out = g.search(qd, k, cap if stop else ef_op, **kw)
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        ids, d, ctr = out
+        return (recall_of(ids.cpu().numpy(), d.cpu().numpy(), ev_d, k), int(ctr[:, 0].sum()),
+                float(np.median(ms)))
+
+    rec_l, dist_l, ms_l = run(True)
+    rec_p, dist_p, ms_p = run(False)
+    info = dict(rec_learned=rec_l, rec_plain=rec_p, dists_learned=dist_l, dists_plain=dist_p,
+                ms_learned=ms_l, ms_plain=ms_p, ef_plain=ef_op)
+    assert rec_l >= target - 0.01 and rec_p >= target - 0.01, info
+    assert dist_l < dist_p, info
+    assert ms_l < 1.10 * ms_p, info
