@@ -84,15 +84,6 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_ADMIT_MASKS
 #define HB_ADMIT_MASKS 1
 #endif
-// Batched admission: rank each new neighbour in the results by a 4-ary search (three independent
-// shared-memory reads per step) instead of a binary search.
-#ifndef HB_KARY_SEARCH
-#define HB_KARY_SEARCH 0
-#endif
-// Pop of the next unexpanded result: one shared-memory round instead of three.
-#ifndef HB_FAST_POP
-#define HB_FAST_POP 0
-#endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
 #define HB_PROF_DECL unsigned long long hb_t = clock64();
@@ -1027,45 +1018,12 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
     const bool inc = (cm >> lane) & 1u;
     int lo = 0, n_eq = 0, eq_lt = 0;
     if (inc) {
-#if HB_KARY_SEARCH
-        // lo: entries of R0 with distance below dj. The answer stays in [a, a + len]; each step
-        // reads three independent split points (one round trip to shared memory) and keeps one
-        // quarter, then a binary search finishes.
-        int a = 0, len = r0;
-        while (len >= 4) {
-            const int q = len >> 2;
-            const int s1 = a + q, s2 = a + 2 * q, s3 = a + 3 * q;
-            const bool b1 = C.Rd[s1] < dj, b2 = C.Rd[s2] < dj, b3 = C.Rd[s3] < dj;
-            if (b3) {
-                len = a + len - s3 - 1;
-                a = s3 + 1;
-            } else if (b2) {
-                a = s2 + 1;
-                len = q - 1;
-            } else if (b1) {
-                a = s1 + 1;
-                len = q - 1;
-            } else {
-                len = q;
-            }
-        }
-        while (len > 0) {
-            const int m = a + (len >> 1);
-            if (C.Rd[m] < dj) {
-                a = m + 1;
-                len = len - (len >> 1) - 1;
-            } else {
-                len >>= 1;
-            }
-        }
-#else
         int a = 0, b = r0;  // lo: entries of R0 with distance below dj
         while (a < b) {
             const int m = (a + b) >> 1;
             if (C.Rd[m] < dj) a = m + 1;
             else b = m;
         }
-#endif
         lo = a;
         for (int i = a; i < r0 && C.Rd[i] == dj; i++) {  // equal distances: rank by id
             n_eq++;
@@ -1215,22 +1173,6 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
         int32_t c = -1;
         while (scan < r) {
             const int i = scan + lane;
-#if HB_FAST_POP
-            // Every lane reads its entry's two ids at once; the first unexpanded lane marks its
-            // entry expanded and its internal id comes by shuffle (the ballot orders these writes
-            // after every lane's read).
-            const int32_t ri = i < r ? C.Ri[i] : EXP_BIT;
-            const int32_t rp = i < r ? C.Rp[i] : 0;
-            const uint32_t b = __ballot_sync(FULL, !(ri & EXP_BIT));
-            if (b) {
-                const int j = __ffs(b) - 1;
-                if (lane == j) C.Ri[i] = ri | EXP_BIT;
-                c = __shfl_sync(FULL, rp, j) & ID_MASK;
-                scan += j + 1;
-                __syncwarp();
-                break;
-            }
-#else
             const bool un = i < r && !(C.Ri[i] & EXP_BIT);
             const uint32_t b = __ballot_sync(FULL, un);
             if (b) {
@@ -1243,7 +1185,6 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
                 __syncwarp();
                 break;
             }
-#endif
             scan += 32;
         }
         if (c < 0) {

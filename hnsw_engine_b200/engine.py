@@ -105,7 +105,9 @@ class CapturedSearch:
     def __init__(self, graph: "DeviceGraph", queries: torch.Tensor, k: int, ef: int, *,
                  stop: tuple | None = None) -> None:
         self.graph = graph
-        self.queries = queries.to(device=graph.device, dtype=torch.float32).contiguous()
+        # the graph reads this buffer: its own copy, never an alias of the caller's tensor
+        self.queries = torch.empty(tuple(queries.shape), dtype=torch.float32, device=graph.device)
+        self.queries.copy_(queries)
         self.k, self.ef, self.stop = int(k), int(ef), stop
         nq = self.queries.shape[0]
         dev = graph.device
