@@ -186,18 +186,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Two float32 lanes per instruction (Blackwell packed f32x2): each half is rounded exactly as the
-// scalar add / fma, so the results are those of fmaf(-2, v, qq + x) element by element.
-__device__ __forceinline__ void fma_l2_pair(float &v0, float &v1, float qq, float x0, float x1) {
-    asm("{\n\t.reg .b64 rq, rx, rs, rv, rm;\n\t"
-        "mov.b64 rq, {%2, %2};\n\tmov.b64 rx, {%3, %4};\n\t"
-        "add.rn.f32x2 rs, rq, rx;\n\t"
-        "mov.b64 rv, {%0, %1};\n\tmov.b64 rm, {%5, %5};\n\t"
-        "fma.rn.f32x2 rv, rm, rv, rs;\n\tmov.b64 {%0, %1}, rv;\n\t}"
-        : "+f"(v0), "+f"(v1)
-        : "f"(qq), "f"(x0), "f"(x1), "f"(-2.f));
-}
-
 __global__ void __launch_bounds__(FILTER_THREADS, 1)
     knn_filter_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const FilterParams p) {
@@ -373,51 +361,49 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 float v[32];
                 tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
                 const int valid = min(32, p.row_end - col0);  // columns that are data rows
-                uint32_t keep = 0;
-                // One loop per metric (the branch is uniform): l2 |q|^2 + |x|^2 - 2 q.x; ip -q.x;
-                // cosine 1 - q.x (normalised rows). Columns past the data rows are masked once.
+                // The filter value is a = v + vadd with v = |x|^2 - 2 q.x (l2), -q.x (ip, cosine)
+                // and vadd = |q|^2, 0, 1: one FMA or negation per element, then the chunk's
+                // minimum. fl(v + vadd) is monotonic in v, so a chunk whose minimum fails the
+                // threshold has no candidate; the rare chunks with one test each element.
                 if (l2) {
 #pragma unroll
-                    for (int j = 0; j < 32; j += 2) {
-                        fma_l2_pair(v[j], v[j + 1], qq, xv[j], xv[j + 1]);
-                        keep |= v[j] <= thr ? (1u << j) : 0u;
-                        keep |= v[j + 1] <= thr ? (2u << j) : 0u;
-                    }
-                } else if (cosine) {
-#pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        v[j] = 1.f - v[j];
-                        keep |= v[j] <= thr ? (1u << j) : 0u;
-                    }
+                    for (int j = 0; j < 32; j++) v[j] = fmaf(-2.f, v[j], xv[j]);
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        v[j] = -v[j];
-                        keep |= v[j] <= thr ? (1u << j) : 0u;
-                    }
+                    for (int j = 0; j < 32; j++) v[j] = -v[j];
                 }
-                if (valid < 32) keep &= valid <= 0 ? 0u : (0xffffffffu >> (32 - valid));
+                if (valid < 32) {  // uniform: only the last tile of the rows
+#pragma unroll
+                    for (int j = 0; j < 32; j++)
+                        if (j >= valid) v[j] = INFINITY;
+                }
+                float m16[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) m16[j] = fminf(v[j], v[j + 16]);
+#pragma unroll
+                for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+                    for (int j = 0; j < w; j++) m16[j] = fminf(m16[j], m16[j + w]);
+                const float vadd = l2 ? qq : (cosine ? 1.f : 0.f);
+                const float amin = m16[0] + vadd;
                 if (p.block_min) {
                     // Threshold pass: the k-th smallest of the blocks' minima is at least the k-th
                     // smallest of all the values (a subset's k-th is never below the set's), so
                     // one candidate per block still bounds the k-th distance from above.
-                    float mn = INFINITY;
-#pragma unroll
-                    for (int j = 0; j < 32; j++)
-                        if ((keep >> j) & 1u) mn = fminf(mn, v[j]);
-                    if (keep && qvalid) {
+                    if (valid > 0 && qvalid && amin <= thr) {
                         if (cnt < p.cap) {
-                            cv[cnt] = mn;
+                            cv[cnt] = amin;
                             ci[cnt] = col0;
                         }
                         cnt++;
                     }
-                } else if (keep && qvalid) {
+                } else if (qvalid && amin <= thr) {
 #pragma unroll
                     for (int j = 0; j < 32; j++) {  // static indices keep v[] in registers
-                        if ((keep >> j) & 1u) {
+                        const float a = v[j] + vadd;
+                        if (j < valid && a <= thr) {
                             if (cnt < p.cap) {
-                                cv[cnt] = v[j];
+                                cv[cnt] = a;
                                 ci[cnt] = col0 + j;
                             }
                             cnt++;
@@ -779,6 +765,13 @@ constexpr int64_t CAND_BYTES = int64_t(4) << 30;
 #define HB_EXPECT_FACTOR 2
 #endif
 constexpr int64_t EXPECT_FACTOR = HB_EXPECT_FACTOR;
+// Pass one reads at least n / PREFIX_DIV rows: a longer prefix gives a tighter tau, so fewer rows
+// pass in pass two (about k * PREFIX_DIV) and the epilogue's per-element path runs on fewer
+// chunks; the prefix costs 1 / PREFIX_DIV of a full pass.
+#ifndef HB_PREFIX_DIV
+#define HB_PREFIX_DIV 8
+#endif
+constexpr int64_t PREFIX_DIV = HB_PREFIX_DIV;
 
 // One attempt at the whole batch with candidate lists of at least cap_min entries. Returns
 // HNSW_B200_ERETRY with *cap_needed set when a query's candidates outgrew its list (many rows
@@ -816,7 +809,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     // prefix of them. Each epilogue thread appends to its own segment of the query's list: at most
     // 3 (block minima) or 96 (rows) entries per tile in pass one; pass two's segments are sized for
     // three times their expected share (an overflow re-runs the call with longer segments).
-    const int64_t prefix = std::min<int64_t>(n, std::max<int64_t>(int64_t(64) * k, 32768));
+    const int64_t prefix =
+        std::min<int64_t>(n, std::max<int64_t>({int64_t(64) * k, int64_t(32768), n / PREFIX_DIV}));
     const bool block_min = (prefix + 31) / 32 >= k;
     const int64_t expect2 = EXPECT_FACTOR * int64_t(k) * ((n + prefix - 1) / prefix) + int64_t(k);
     int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
