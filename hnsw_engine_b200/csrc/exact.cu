@@ -496,9 +496,16 @@ __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32
     const int q = blockIdx.x;
     if (q >= nq) return;
     const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
-    int m = 0;
-    for (int sg = 0; sg < nseg; sg++) m += min(cnt[sg], cap);
+    __shared__ int s_m;
+    if (threadIdx.x == 0) s_m = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int sg = threadIdx.x; sg < nseg; sg += blockDim.x) mine += min(cnt[sg], cap);
+    atomicAdd(&s_m, mine);
+    __syncthreads();
+    const int m = s_m;
     const float *v = cand_val + int64_t(q) * nseg * cap;
+    const int wid = threadIdx.x >> 5, lid = threadIdx.x & 31;
     if (m < k) {
         if (threadIdx.x == 0) {
             out_tau[q] = INFINITY;
@@ -511,9 +518,9 @@ __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32
         for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
         __syncthreads();
         const uint32_t hmask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
-        for (int sg = 0; sg < nseg; sg++) {
+        for (int sg = wid; sg < nseg; sg += int(blockDim.x >> 5)) {  // a warp per segment
             const int ms = min(cnt[sg], cap);
-            for (int i = threadIdx.x; i < ms; i += blockDim.x) {
+            for (int i = lid; i < ms; i += 32) {
                 const uint32_t key = fkey(v[int64_t(sg) * cap + i]);
                 if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
             }
@@ -576,14 +583,29 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
     const double qn = qnorm[q];
     int a = 0;
     double err = 0.0;  // largest |filter value - exact distance| over this lane's survivors
-    for (int sg = 0; sg < nseg; sg++) {
-    const int m = min(cand_cnt[int64_t(q) * nseg + sg], cap);
-    const int64_t sb = (int64_t(q) * nseg + sg) * cap;
-    for (int base = 0; base < m; base += 32) {
-        const int i = base + lane;
-        const float approx = i < m ? cand_val[sb + i] : INFINITY;
-        bool has = i < m && approx <= t;
-        int32_t id = has ? cand_id[sb + i] : -1;
+    // Batches of 32 candidates taken across the segments in order, so every lane scores one
+    // (segments hold a few entries each).
+    const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
+    int sg = 0, off = 0;
+    while (sg < nseg && min(cnt[sg], cap) == 0) sg++;
+    while (sg < nseg) {
+        int64_t at = -1;  // this lane's entry
+        int filled = 0;
+        while (filled < 32 && sg < nseg) {  // uniform
+            const int c = min(cnt[sg], cap);
+            const int take = min(c - off, 32 - filled);
+            if (lane >= filled && lane < filled + take) at = (int64_t(q) * nseg + sg) * cap + off + (lane - filled);
+            filled += take;
+            off += take;
+            if (off >= c) {
+                off = 0;
+                sg++;
+                while (sg < nseg && min(cnt[sg], cap) == 0) sg++;
+            }
+        }
+        const float approx = at >= 0 ? cand_val[at] : INFINITY;
+        bool has = at >= 0 && approx <= t;
+        int32_t id = has ? cand_id[at] : -1;
         double d = INFINITY;
         if (has) {
             const T *x = data + int64_t(id) * dim;
@@ -637,7 +659,6 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
             __syncwarp();
             a = min(a + 1, k);
         }
-    }
     }
     for (int r = lane; r < k; r += 32) {
         out_ids[int64_t(q) * k + r] = r < a ? int64_t(Ai[r]) : -1;

@@ -718,6 +718,43 @@ __device__ __forceinline__ void score_chunk(const SearchParams &P, Cx &C, int32_
     dj = typename Cx::dist_t(d);
 }
 
+// Distance of a byte row held in registers (v4 16-byte words) to the byte query in shared memory:
+// L2 sums |x - q|^2 by __vabsdiffu4 + __dp4a, inner product sums x.q by __dp4a. Four independent
+// integer accumulators (one per 32-bit word of a 16-byte load) keep the dependent chain at a
+// quarter of its length; integer sums, so the value is the same in any order.
+template <typename D, class Cx>
+__device__ __forceinline__ D row_dot_bytes(const SearchParams &P, const Cx &C, const uint4 (&x)[8],
+                                           int v4) {
+    const uint4 *qv = reinterpret_cast<const uint4 *>(C.q4);
+    uint32_t a0 = 0u, a1 = 0u, a2 = 0u, a3 = 0u;
+    if (P.metric == HNSW_B200_L2) {
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            if (t < v4) {
+                const uint4 q = qv[t];
+                const uint32_t d0 = __vabsdiffu4(x[t].x, q.x), d1 = __vabsdiffu4(x[t].y, q.y);
+                const uint32_t d2 = __vabsdiffu4(x[t].z, q.z), d3 = __vabsdiffu4(x[t].w, q.w);
+                a0 = __dp4a(d0, d0, a0);
+                a1 = __dp4a(d1, d1, a1);
+                a2 = __dp4a(d2, d2, a2);
+                a3 = __dp4a(d3, d3, a3);
+            }
+        }
+        return D((a0 + a1) + (a2 + a3));
+    }
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+        if (t < v4) {
+            const uint4 q = qv[t];
+            a0 = __dp4a(x[t].x, q.x, a0);
+            a1 = __dp4a(x[t].y, q.y, a1);
+            a2 = __dp4a(x[t].z, q.z, a2);
+            a3 = __dp4a(x[t].w, q.w, a3);
+        }
+    }
+    return -D((a0 + a1) + (a2 + a3));
+}
+
 // Byte rows of at most 128 bytes starting on 16-byte boundaries (dim a multiple of 16): every lane
 // loads the whole row of the neighbour it holds -- eight 16-byte loads in flight per lane -- before
 // the visited marks are resolved, so the gather overlaps the marking atomics and all rows of a chunk
@@ -736,39 +773,7 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, 
     for (int t = 0; t < 8; t++) x[t] = (e >= 0 && t < v4) ? __ldg(row + t) : make_uint4(0u, 0u, 0u, 0u);
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
     dj = D(0);
-    if ((um >> C.lane) & 1u) {
-        const uint4 *qv = reinterpret_cast<const uint4 *>(C.q4);
-        uint32_t acc = 0u;
-        if (P.metric == HNSW_B200_L2) {
-#pragma unroll
-            for (int t = 0; t < 8; t++) {
-                if (t < v4) {
-                    const uint4 q = qv[t];
-                    uint32_t d = __vabsdiffu4(x[t].x, q.x);
-                    acc = __dp4a(d, d, acc);
-                    d = __vabsdiffu4(x[t].y, q.y);
-                    acc = __dp4a(d, d, acc);
-                    d = __vabsdiffu4(x[t].z, q.z);
-                    acc = __dp4a(d, d, acc);
-                    d = __vabsdiffu4(x[t].w, q.w);
-                    acc = __dp4a(d, d, acc);
-                }
-            }
-            dj = D(acc);
-        } else {
-#pragma unroll
-            for (int t = 0; t < 8; t++) {
-                if (t < v4) {
-                    const uint4 q = qv[t];
-                    acc = __dp4a(x[t].x, q.x, acc);
-                    acc = __dp4a(x[t].y, q.y, acc);
-                    acc = __dp4a(x[t].z, q.z, acc);
-                    acc = __dp4a(x[t].w, q.w, acc);
-                }
-            }
-            dj = -D(acc);
-        }
-    }
+    if ((um >> C.lane) & 1u) dj = row_dot_bytes<D>(P, C, x, v4);
     return um;
 }
 
@@ -804,40 +809,11 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows_staged(const SearchPara
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     dj = D(0);
     if ((um >> C.lane) & 1u) {
-        const uint4 *qv = reinterpret_cast<const uint4 *>(C.q4);
         const uint4 *xs = reinterpret_cast<const uint4 *>(mine);
-        uint32_t acc = 0u;
-        if (P.metric == HNSW_B200_L2) {
+        uint4 x[8];
 #pragma unroll
-            for (int t = 0; t < 8; t++) {
-                if (t < v4) {
-                    const uint4 q = qv[t];
-                    const uint4 x = xs[t ^ sw];
-                    uint32_t d = __vabsdiffu4(x.x, q.x);
-                    acc = __dp4a(d, d, acc);
-                    d = __vabsdiffu4(x.y, q.y);
-                    acc = __dp4a(d, d, acc);
-                    d = __vabsdiffu4(x.z, q.z);
-                    acc = __dp4a(d, d, acc);
-                    d = __vabsdiffu4(x.w, q.w);
-                    acc = __dp4a(d, d, acc);
-                }
-            }
-            dj = D(acc);
-        } else {
-#pragma unroll
-            for (int t = 0; t < 8; t++) {
-                if (t < v4) {
-                    const uint4 q = qv[t];
-                    const uint4 x = xs[t ^ sw];
-                    acc = __dp4a(x.x, q.x, acc);
-                    acc = __dp4a(x.y, q.y, acc);
-                    acc = __dp4a(x.z, q.z, acc);
-                    acc = __dp4a(x.w, q.w, acc);
-                }
-            }
-            dj = -D(acc);
-        }
+        for (int t = 0; t < 8; t++) x[t] = t < v4 ? xs[t ^ sw] : make_uint4(0u, 0u, 0u, 0u);
+        dj = row_dot_bytes<D>(P, C, x, v4);
     }
     return um;
 }
