@@ -45,11 +45,18 @@ constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;
 constexpr int B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-// Epilogue warps: EPI_WARPS / 4 per TMEM lane quarter, taking a tile's 32-column chunks in turn.
+// Epilogue warps: EPI_WARPS / 4 per TMEM lane quarter, taking a tile's CW-column chunks in turn.
+// Narrower chunks need fewer registers per thread, which leaves room for more epilogue warps to
+// hide the TMEM-load and arithmetic latencies.
 #ifndef HB_EPI_WARPS
-#define HB_EPI_WARPS 12
+#define HB_EPI_WARPS 20
+#endif
+#ifndef HB_EPI_CW
+#define HB_EPI_CW 16
 #endif
 constexpr int EPI_WARPS = HB_EPI_WARPS;
+constexpr int CW = HB_EPI_CW;  // columns per TMEM load (16 or 32)
+static_assert(CW == 16 || CW == 32, "chunks of 16 or 32 columns");
 constexpr int EPI_PER_QUARTER = EPI_WARPS / 4;
 constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
 constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
@@ -78,7 +85,7 @@ struct FilterParams {
     int32_t *cand_id;      // (nq, nseg, cap) row ids
     int32_t *cand_cnt;     // (nq, nseg) appended counts (may exceed cap: overflow)
     int32_t cap;           // entries per segment
-    int32_t block_min;     // 1: append only the minimum of each 32-row block (the threshold pass)
+    int32_t block_min;     // 1: append only the minimum of each CW-row block (the threshold pass)
     int32_t *err;          // nonzero: a bounded wait expired
 };
 
@@ -184,6 +191,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+template <int W>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[W]) {
+    if constexpr (W == 16) tmem_ld16(taddr, v);
+    else tmem_ld32(taddr, v);
 }
 
 __global__ void __launch_bounds__(FILTER_THREADS, 1)
@@ -341,16 +368,16 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int row0 = p.row_begin + (t0 + lt) * BN;
 #pragma unroll 1
-            for (int c = part * 32; c < BN; c += 32 * EPI_PER_QUARTER) {
+            for (int c = part * CW; c < BN; c += CW * EPI_PER_QUARTER) {
                 const int col0 = row0 + c;
-                // |x|^2 of the 32 columns: the same addresses in every lane (broadcast loads),
-                // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + 32
+                // |x|^2 of the CW columns: the same addresses in every lane (broadcast loads),
+                // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + CW
                 // entries (zero beyond the data rows).
-                float xv[32];
+                float xv[CW];
                 if (l2) {
                     const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
 #pragma unroll
-                    for (int i = 0; i < 8; i++) {
+                    for (int i = 0; i < CW / 4; i++) {
                         const float4 t = __ldg(x4 + i);
                         xv[4 * i] = t.x;
                         xv[4 * i + 1] = t.y;
@@ -358,34 +385,34 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                         xv[4 * i + 3] = t.w;
                     }
                 }
-                float v[32];
-                tmem_ld32(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
-                const int valid = min(32, p.row_end - col0);  // columns that are data rows
+                float v[CW];
+                tmem_ld<CW>(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
+                const int valid = min(CW, p.row_end - col0);  // columns that are data rows
                 // The filter value is a = v + vadd with v = |x|^2 - 2 q.x (l2), -q.x (ip, cosine)
                 // and vadd = |q|^2, 0, 1: one FMA or negation per element, then the chunk's
                 // minimum. fl(v + vadd) is monotonic in v, so a chunk whose minimum fails the
                 // threshold has no candidate; the rare chunks with one test each element.
                 if (l2) {
 #pragma unroll
-                    for (int j = 0; j < 32; j++) v[j] = fmaf(-2.f, v[j], xv[j]);
+                    for (int j = 0; j < CW; j++) v[j] = fmaf(-2.f, v[j], xv[j]);
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 32; j++) v[j] = -v[j];
+                    for (int j = 0; j < CW; j++) v[j] = -v[j];
                 }
-                if (valid < 32) {  // uniform: only the last tile of the rows
+                if (valid < CW) {  // uniform: only the last tile of the rows
 #pragma unroll
-                    for (int j = 0; j < 32; j++)
+                    for (int j = 0; j < CW; j++)
                         if (j >= valid) v[j] = INFINITY;
                 }
-                float m16[16];
+                float mh[CW / 2];
 #pragma unroll
-                for (int j = 0; j < 16; j++) m16[j] = fminf(v[j], v[j + 16]);
+                for (int j = 0; j < CW / 2; j++) mh[j] = fminf(v[j], v[j + CW / 2]);
 #pragma unroll
-                for (int w = 8; w > 0; w >>= 1)
+                for (int w = CW / 4; w > 0; w >>= 1)
 #pragma unroll
-                    for (int j = 0; j < w; j++) m16[j] = fminf(m16[j], m16[j + w]);
+                    for (int j = 0; j < w; j++) mh[j] = fminf(mh[j], mh[j + w]);
                 const float vadd = l2 ? qq : (cosine ? 1.f : 0.f);
-                const float amin = m16[0] + vadd;
+                const float amin = mh[0] + vadd;
                 if (p.block_min) {
                     // Threshold pass: the k-th smallest of the blocks' minima is at least the k-th
                     // smallest of all the values (a subset's k-th is never below the set's), so
@@ -399,7 +426,7 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                     }
                 } else if (qvalid && amin <= thr) {
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {  // static indices keep v[] in registers
+                    for (int j = 0; j < CW; j++) {  // static indices keep v[] in registers
                         const float a = v[j] + vadd;
                         if (j < valid && a <= thr) {
                             if (cnt < p.cap) {
@@ -779,9 +806,10 @@ size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Candidate lists take at most CAND_BYTES of scratch: (query, segment) pairs x cap x 8 bytes.
 constexpr int64_t CAND_BYTES = int64_t(4) << 30;
-// Pass two keeps about k n / prefix rows per query: tau is the k-th smallest of the prefix's 32-row
-// block minima, a loose upper bound of the k-th distance (3,244 per query measured for k = 100 on the
-// 1M x 128 mixture, against 3,100 for k n / prefix). Lists are sized for EXPECT_FACTOR times that.
+// Pass two keeps about k n / prefix rows per query: tau is the k-th smallest of the prefix's CW-row
+// block minima, a loose upper bound of the k-th distance (830 per query measured for k = 100 on the
+// 1M x 128 mixture with a prefix of n / 8, against 800 for k n / prefix). Lists are sized for
+// EXPECT_FACTOR times that.
 #ifndef HB_EXPECT_FACTOR
 #define HB_EXPECT_FACTOR 2
 #endif
@@ -825,14 +853,15 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         g.splits = (tiles + g.tps - 1) / g.tps;
         return g;
     };
-    // Pass one keeps the minimum of every 32-row block of a prefix (every row when the prefix has
+    // Pass one keeps the minimum of every CW-row block of a prefix (every row when the prefix has
     // fewer than k blocks); pass two keeps the rows within tau + margin, about EXPECT_FACTOR k n /
     // prefix of them. Each epilogue thread appends to its own segment of the query's list: at most
-    // 3 (block minima) or 96 (rows) entries per tile in pass one; pass two's segments are sized for
-    // three times their expected share (an overflow re-runs the call with longer segments).
+    // one entry (block minima) or CW (rows) per chunk it takes of a tile in pass one; pass two's
+    // segments are sized for three times their expected share (an overflow re-runs the call with
+    // longer segments).
     const int64_t prefix =
         std::min<int64_t>(n, std::max<int64_t>({int64_t(64) * k, int64_t(32768), n / PREFIX_DIV}));
-    const bool block_min = (prefix + 31) / 32 >= k;
+    const bool block_min = (prefix + CW - 1) / CW >= k;
     const int64_t expect2 = EXPECT_FACTOR * int64_t(k) * ((n + prefix - 1) / prefix) + int64_t(k);
     int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
     int64_t cap = 0, slots = 0;                      // entries per segment; (query, segment) pairs
@@ -843,7 +872,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         for (int64_t nqc : {QB, last}) {
             const Geo g1 = geo(nqc, prefix), g2 = geo(nqc, n);
             const int64_t nseg2 = int64_t(g2.splits) * EPI_PER_QUARTER;
-            cap = std::max<int64_t>(cap, int64_t(block_min ? 3 : 96) * g1.tps);
+            const int64_t per_tile = (BN / CW + EPI_PER_QUARTER - 1) / EPI_PER_QUARTER;  // chunks
+            cap = std::max<int64_t>(cap, per_tile * (block_min ? 1 : CW) * g1.tps);
             cap = std::max<int64_t>(cap, (3 * expect2 + nseg2 - 1) / nseg2 + 32);
             slots = std::max<int64_t>(slots, nqc * std::max(g1.splits, g2.splits) * EPI_PER_QUARTER);
         }
@@ -964,7 +994,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         };
         // Pass one: the prefix rows with no threshold give tau (an upper bound of the k-th).
         XT(cudaMemcpyAsync(th, inf.data(), size_t(nq) * 4, cudaMemcpyHostToDevice, s));
-        // One candidate per 32-row block suffices while the prefix has at least k blocks.
+        // One candidate per CW-row block suffices while the prefix has at least k blocks.
         if (int rc = run_filter(prefix, block_min)) return rc;
         select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg,
                                            th, tau);
