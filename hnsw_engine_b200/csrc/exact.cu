@@ -859,8 +859,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     // one entry (block minima) or CW (rows) per chunk it takes of a tile in pass one; pass two's
     // segments are sized for three times their expected share (an overflow re-runs the call with
     // longer segments).
-    const int64_t prefix =
-        std::min<int64_t>(n, std::max<int64_t>({int64_t(64) * k, int64_t(32768), n / PREFIX_DIV}));
+    const int64_t prefix = std::min<int64_t>(n, std::max<int64_t>(int64_t(64) * k, n / PREFIX_DIV));
     const bool block_min = (prefix + CW - 1) / CW >= k;
     const int64_t expect2 = EXPECT_FACTOR * int64_t(k) * ((n + prefix - 1) / prefix) + int64_t(k);
     int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
