@@ -59,6 +59,10 @@ constexpr int CW = HB_EPI_CW;  // columns per TMEM load (16 or 32)
 static_assert(CW == 16 || CW == 32, "chunks of 16 or 32 columns");
 constexpr int EPI_PER_QUARTER = EPI_WARPS / 4;
 constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
+// Shared memory after the stage buffers: barriers and flags (BAR_BYTES), then every epilogue warp's
+// |x|^2 staging for its chunks of a tile (XW floats: at most ceil(BN / CW / parts) chunks of CW).
+constexpr int BAR_BYTES = 256;
+constexpr int XW = ((BN / CW + EPI_PER_QUARTER - 1) / EPI_PER_QUARTER) * CW;
 constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s
 
@@ -353,8 +357,22 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         int cnt = 0;  // this thread's appends (its own segment: no atomics)
         const bool l2 = p.metric == HNSW_B200_L2;
         const bool cosine = p.metric == HNSW_B200_COSINE;
+        // |x|^2 of this warp's chunks of the current tile (XW floats of shared memory per warp),
+        // loaded before the warp waits for the tile's accumulator, so their latency overlaps it.
+        float *xw = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES + BAR_BYTES) + (warp - 4) * XW;
+        const int my_chunks = (BN / CW - part + EPI_PER_QUARTER - 1) / EPI_PER_QUARTER;
         for (int lt = 0; lt < ntiles; lt++) {
             const int b = lt & 1;
+            const int row0 = p.row_begin + (t0 + lt) * BN;
+            if (l2) {
+                if (lane < my_chunks * (CW / 4)) {  // xx holds n_pad >= row0 + BN entries
+                    const int ch = lane / (CW / 4), qd = lane % (CW / 4);
+                    const int col = (part + ch * EPI_PER_QUARTER) * CW + qd * 4;
+                    reinterpret_cast<float4 *>(xw)[lane] =
+                        __ldg(reinterpret_cast<const float4 *>(p.xx + row0 + col));
+                }
+                __syncwarp();
+            }
             int ok = 1;
             if (lane == 0) ok = mbar_wait(tfull + b, (lt >> 1) & 1, abort_flag) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -366,19 +384,16 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int row0 = p.row_begin + (t0 + lt) * BN;
 #pragma unroll 1
-            for (int c = part * CW; c < BN; c += CW * EPI_PER_QUARTER) {
+            for (int c = part * CW, ch = 0; c < BN; c += CW * EPI_PER_QUARTER, ch++) {
                 const int col0 = row0 + c;
-                // |x|^2 of the CW columns: the same addresses in every lane (broadcast loads),
-                // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + CW
-                // entries (zero beyond the data rows).
+                // |x|^2 of the CW columns from this warp's staging (shared-memory broadcasts).
                 float xv[CW];
                 if (l2) {
-                    const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
+                    const float4 *x4 = reinterpret_cast<const float4 *>(xw + ch * CW);
 #pragma unroll
                     for (int i = 0; i < CW / 4; i++) {
-                        const float4 t = __ldg(x4 + i);
+                        const float4 t = x4[i];
                         xv[4 * i] = t.x;
                         xv[4 * i + 1] = t.y;
                         xv[4 * i + 2] = t.z;
@@ -941,7 +956,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     CUtensorMap tmA, tmB;
     if (int rc = make_map(&tmA, qb, q_pad, kp, BM)) return rc;
     if (int rc = make_map(&tmB, xb, n_pad, kp, BN)) return rc;
-    const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
+    const size_t smem = STAGES * STAGE_BYTES + 1024 + BAR_BYTES + size_t(EPI_WARPS) * XW * 4;
     XT(cudaFuncSetAttribute(knn_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int wpb = 4;
     const size_t rsm = size_t(wpb) * (k + 1) * 12;
