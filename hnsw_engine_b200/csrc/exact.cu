@@ -28,6 +28,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "hnsw_b200.h"
@@ -63,6 +64,8 @@ constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
 // |x|^2 staging for its chunks of a tile (XW floats: at most ceil(BN / CW / parts) chunks of CW).
 constexpr int BAR_BYTES = 256;
 constexpr int XW = ((BN / CW + EPI_PER_QUARTER - 1) / EPI_PER_QUARTER) * CW;
+// Rows of at least COOP_DIM dimensions are re-scored by the whole warp, one candidate at a time.
+constexpr int COOP_DIM = 256;
 constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
 constexpr unsigned long long WAIT_LIMIT_NS = 4000000000ull;  // 4 s
 
@@ -528,28 +531,24 @@ __device__ __forceinline__ float funkey(uint32_t k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-// One block of 256 threads per query: tau[q] = k-th smallest of the candidate values (or +inf if
-// fewer than k), then out_thr[q] = tau + margin[q].
+// One warp per query, 8 per block: tau[q] = k-th smallest of the candidate values (or +inf if
+// fewer than k), then out_thr[q] = tau + margin[q]. A 4-pass radix select, 8 bits a pass, over the
+// query's segments; the bin of the rank-th key comes from each lane's 8 bins and a warp scan.
+constexpr int SELECT_WARPS = 8;
 __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32_t cap, int32_t nseg,
                            int32_t nq, int32_t k, const float *margin, float *out_thr, float *out_tau) {
-    __shared__ uint32_t hist[256];
-    __shared__ uint32_t wsum[8];  // per-warp bin totals (blockDim.x == 256)
-    __shared__ uint32_t s_prefix, s_rank;
-    const int q = blockIdx.x;
-    if (q >= nq) return;
+    __shared__ uint32_t hist_all[SELECT_WARPS][256];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q = blockIdx.x * SELECT_WARPS + wid;
+    if (q >= nq) return;  // no block-wide barrier below
+    uint32_t *hist = hist_all[wid];
     const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
-    __shared__ int s_m;
-    if (threadIdx.x == 0) s_m = 0;
-    __syncthreads();
-    int mine = 0;
-    for (int sg = threadIdx.x; sg < nseg; sg += blockDim.x) mine += min(cnt[sg], cap);
-    atomicAdd(&s_m, mine);
-    __syncthreads();
-    const int m = s_m;
+    int m = 0;
+    for (int sg = lane; sg < nseg; sg += 32) m += min(cnt[sg], cap);
+    m = __reduce_add_sync(0xffffffffu, m);
     const float *v = cand_val + int64_t(q) * nseg * cap;
-    const int wid = threadIdx.x >> 5, lid = threadIdx.x & 31;
     if (m < k) {
-        if (threadIdx.x == 0) {
+        if (lane == 0) {
             out_tau[q] = INFINITY;
             out_thr[q] = INFINITY;
         }
@@ -557,42 +556,49 @@ __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32
     }
     uint32_t prefix = 0, rank = uint32_t(k);  // rank: 1-based position within the current bucket
     for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
-        __syncthreads();
+        for (int i = lane; i < 256; i += 32) hist[i] = 0;
+        __syncwarp();
         const uint32_t hmask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
-        for (int sg = wid; sg < nseg; sg += int(blockDim.x >> 5)) {  // a warp per segment
+        for (int sg = 0; sg < nseg; sg++) {
             const int ms = min(cnt[sg], cap);
-            for (int i = lid; i < ms; i += 32) {
+            for (int i = lane; i < ms; i += 32) {
                 const uint32_t key = fkey(v[int64_t(sg) * cap + i]);
                 if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
             }
         }
-        __syncthreads();
-        // The bucket holding the rank-th key: the bin whose counts before it are below rank and
-        // through it reach rank. A prefix sum over the 256 bins (one per thread: a warp scan,
-        // then the 8 warp totals), so exactly one thread finds it.
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        const uint32_t c = hist[threadIdx.x];
-        uint32_t incl = c;
+        __syncwarp();
+        uint32_t c[8], sum = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            c[b] = hist[lane * 8 + b];
+            sum += c[b];
+        }
+        uint32_t incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        if (lane == 31) wsum[warp] = incl;
-        __syncthreads();
-        for (int w = 0; w < warp; w++) incl += wsum[w];
-        const uint32_t excl = incl - c;
-        if (excl < rank && rank <= incl) {
-            s_prefix = prefix | (uint32_t(threadIdx.x) << shift);
-            s_rank = rank - excl;
+        uint32_t run = incl - sum, bucket = 0, nrank = 0;
+        const bool mine = run < rank && rank <= incl;  // exactly one lane
+        if (mine) {
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                if (nrank == 0 && run + c[b] >= rank) {
+                    bucket = uint32_t(lane * 8 + b);
+                    nrank = rank - run;
+                }
+                run += c[b];
+            }
         }
-        __syncthreads();
-        prefix = s_prefix;
-        rank = s_rank;
-        __syncthreads();
+        const int src = __ffs(__ballot_sync(0xffffffffu, mine)) - 1;
+        bucket = __shfl_sync(0xffffffffu, bucket, src);
+        nrank = __shfl_sync(0xffffffffu, nrank, src);
+        prefix |= bucket << shift;
+        rank = nrank;
+        __syncwarp();
     }
-    if (threadIdx.x == 0) {
+    if (lane == 0) {
         const float tau = funkey(prefix);
         out_tau[q] = tau;
         out_thr[q] = tau + margin[q];
@@ -649,7 +655,37 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
         bool has = at >= 0 && approx <= t;
         int32_t id = has ? cand_id[at] : -1;
         double d = INFINITY;
-        if (has) {
+        if (dim >= COOP_DIM) {
+            // Long rows: the warp scores the batch's candidates one after another, each lane
+            // summing every 32nd dimension and a fixed shuffle tree adding the lanes (the same value
+            // on every run; on integer data every order gives the same exact sum), so the float64
+            // chains are 32 times shorter than one lane per candidate.
+            for (uint32_t hm = __ballot_sync(0xffffffffu, has); hm; hm &= hm - 1) {
+                const int j = __ffs(hm) - 1;
+                const int32_t idj = __shfl_sync(0xffffffffu, id, j);
+                const T *x = data + int64_t(idj) * dim;
+                double acc = 0.0;
+                if (metric == HNSW_B200_L2) {
+                    for (int i = lane; i < dim; i += 32) {
+                        const double df = __dsub_rn(double(x[i]), double(qv[i]));
+                        acc = __dadd_rn(acc, __dmul_rn(df, df));
+                    }
+                } else if (metric == HNSW_B200_IP) {
+                    for (int i = lane; i < dim; i += 32)
+                        acc = __dadd_rn(acc, __dmul_rn(double(x[i]), double(qv[i])));
+                } else {
+                    const double xn = xnorm[idj];
+                    for (int i = lane; i < dim; i += 32)
+                        acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[i]), xn),
+                                                       __ddiv_rn(double(qv[i]), qn)));
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+                if (lane == j)
+                    d = metric == HNSW_B200_L2 ? acc : (metric == HNSW_B200_IP ? -acc : __dsub_rn(1.0, acc));
+            }
+            if (has) err = fmax(err, fabs(double(approx) - d));
+        } else if (has) {
             const T *x = data + int64_t(id) * dim;
             double acc = 0.0;
             if (metric == HNSW_B200_L2) {
@@ -712,6 +748,17 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) eb = max(eb, __shfl_xor_sync(0xffffffffu, eb, o));
     if (lane == 0 && eb) atomicMax(err_max, eb);
+}
+
+// Whether every value is an integer with |v| <= 256 (exact in BF16): *flag gets 1 when one is not.
+__global__ void check_small_int(const float *x, int64_t count, int32_t *flag) {
+    bool bad = false;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        const float v = x[i];
+        bad |= !(v == rintf(v) && fabsf(v) <= 256.f);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 // Largest and total of the segment counts (overflow check and the candidate total).
@@ -829,13 +876,13 @@ constexpr int64_t CAND_BYTES = int64_t(4) << 30;
 #define HB_EXPECT_FACTOR 2
 #endif
 constexpr int64_t EXPECT_FACTOR = HB_EXPECT_FACTOR;
-// Pass one reads at least n / PREFIX_DIV rows: a longer prefix gives a tighter tau, so fewer rows
-// pass in pass two (about k * PREFIX_DIV) and the epilogue's per-element path runs on fewer
-// chunks; the prefix costs 1 / PREFIX_DIV of a full pass.
-#ifndef HB_PREFIX_DIV
-#define HB_PREFIX_DIV 8
-#endif
-constexpr int64_t PREFIX_DIV = HB_PREFIX_DIV;
+// Prefix length. Pass one costs the prefix's rows on the tensor cores; pass two then keeps about
+// k n / prefix rows per query, each re-scored in float64 (and a per-element epilogue path on the
+// chunks holding them). A float64 re-score of a row costs about PREFIX_BALANCE times a row of
+// tensor-core filter work, so the prefix balancing the two is sqrt(PREFIX_BALANCE k n): 122K rows
+// for k = 100 over 1M rows (830 candidates per query), 30K over 60K rows.
+constexpr double PREFIX_BALANCE = 150.0;
+
 
 // One attempt at the whole batch with candidate lists of at least cap_min entries. Returns
 // HNSW_B200_ERETRY with *cap_needed set when a query's candidates outgrew its list (many rows
@@ -845,7 +892,24 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
                     int64_t *cap_needed) {
     const int64_t n = a->n, nq_all = a->nq;
     const int dim = a->dim, k = a->k, metric = a->metric;
-    const int terms = a->integer_valued && metric != HNSW_B200_COSINE ? 1 : 3;
+    int integer = a->integer_valued;
+    if (integer < 0) {  // find out on the device: bytes always are; floats by one pass each
+        integer = 1;
+        if constexpr (std::is_same_v<T, float>) {
+            static thread_local Scratch flag_buf;
+            if (int rc = flag_buf.get(16)) return rc;
+            int32_t *flag = static_cast<int32_t *>(flag_buf.p);
+            XT(cudaMemsetAsync(flag, 0, 4, s));
+            check_small_int<<<1024, 256, 0, s>>>(static_cast<const float *>(a->data), n * dim, flag);
+            check_small_int<<<256, 256, 0, s>>>(static_cast<const float *>(a->queries), nq_all * dim, flag);
+            XT(cudaGetLastError());
+            int32_t hflag = 0;
+            XT(cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s));
+            XT(cudaStreamSynchronize(s));
+            integer = hflag ? 0 : 1;
+        }
+    }
+    const int terms = integer && metric != HNSW_B200_COSINE ? 1 : 3;
     const int seg = (dim + BK - 1) / BK * BK;
     const int kp = seg * terms;
     const int64_t n_pad = (n + BN - 1) / BN * BN;
@@ -874,7 +938,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     // one entry (block minima) or CW (rows) per chunk it takes of a tile in pass one; pass two's
     // segments are sized for three times their expected share (an overflow re-runs the call with
     // longer segments).
-    const int64_t prefix = std::min<int64_t>(n, std::max<int64_t>(int64_t(64) * k, n / PREFIX_DIV));
+    const int64_t prefix = std::min<int64_t>(
+        n, std::max<int64_t>(int64_t(64) * k, int64_t(std::sqrt(PREFIX_BALANCE * double(k) * double(n)))));
     const bool block_min = (prefix + CW - 1) / CW >= k;
     const int64_t expect2 = EXPECT_FACTOR * int64_t(k) * ((n + prefix - 1) / prefix) + int64_t(k);
     int64_t QB = std::min<int64_t>(nq_all, 8192);  // queries per chunk
@@ -1010,8 +1075,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         XT(cudaMemcpyAsync(th, inf.data(), size_t(nq) * 4, cudaMemcpyHostToDevice, s));
         // One candidate per CW-row block suffices while the prefix has at least k blocks.
         if (int rc = run_filter(prefix, block_min)) return rc;
-        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg,
-                                           th, tau);
+        select_kth<<<int((nq + SELECT_WARPS - 1) / SELECT_WARPS), 32 * SELECT_WARPS, 0, s>>>(
+            cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg, th, tau);
         // Pass two: every row against tau + margin.
         if (int rc = run_filter(n, false)) return rc;
         XT(cudaMemsetAsync(cstat, 0, 16, s));
@@ -1033,8 +1098,8 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
                                               " > " + std::to_string(cap) + ")");
         }
         // The k-th smallest candidate is the global k-th approximate distance: final threshold.
-        select_kth<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg,
-                                           th, tau);
+        select_kth<<<int((nq + SELECT_WARPS - 1) / SELECT_WARPS), 32 * SELECT_WARPS, 0, s>>>(
+            cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg, th, tau);
         rerank_topk<T><<<int((nq + wpb - 1) / wpb), wpb * 32, rsm, s>>>(
             X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), int32_t(nseg), th,
             a->out_ids + q0 * k, a->out_dists + q0 * k, ferr);

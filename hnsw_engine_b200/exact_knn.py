@@ -29,17 +29,6 @@ class ExactStats:
     filter_error_bound: float  # derived bound of the filter's error (margins are twice it)
 
 
-def _integer_small(a: Any) -> bool:
-    if isinstance(a, torch.Tensor):
-        if not a.is_floating_point():
-            return bool((a.abs() <= 256).all().item())
-        return bool(((a == a.round()) & (a.abs() <= 256)).all().item())
-    arr = np.asarray(a)
-    if np.issubdtype(arr.dtype, np.integer):
-        return bool(np.abs(arr.astype(np.int64)).max(initial=0) <= 256)
-    return bool(np.array_equal(arr, np.rint(arr)) and np.abs(arr).max(initial=0) <= 256)
-
-
 def exact_search(
     data: Any, queries: Any, k: int, metric: str = "l2", *, device: str | torch.device = "cuda",
     return_stats: bool = False,
@@ -61,7 +50,6 @@ def exact_search(
             raise ValueError(f"data must be non-empty with at least one dimension, got {x_np.shape}")
         q_np = as_matrix(queries, "queries", dim=dim)
         k = check_k(k, n)
-        integer = _integer_small(x_np) and _integer_small(q_np)
         if x_np.dtype == np.uint8 and q_np.dtype == np.uint8:
             x = torch.from_numpy(np.ascontiguousarray(x_np)).to(dev)
             q = torch.from_numpy(np.ascontiguousarray(q_np)).to(dev)
@@ -80,7 +68,6 @@ def exact_search(
         x, q = data.contiguous(), queries.to(dev).contiguous()
         n, dim = x.shape
         k = check_k(k, n)
-        integer = _integer_small(x) and _integer_small(q)
         if not (x.dtype == torch.uint8 and q.dtype == torch.uint8):
             x, q = x.to(torch.float32), q.to(torch.float32)
     nq = q.shape[0]
@@ -93,7 +80,7 @@ def exact_search(
     args = _lib.ExactArgs(
         data=x.data_ptr(), queries=q.data_ptr(),
         dtype=_lib_dtype(x), dim=dim, n=n, nq=nq, k=k, metric=_lib.METRIC_CODES[metric],
-        integer_valued=int(integer), reserved=0, out_ids=ids.data_ptr(), out_dists=dists.data_ptr(),
+        integer_valued=-1, reserved=0, out_ids=ids.data_ptr(), out_dists=dists.data_ptr(),
         out_filter_max_error=ctypes.addressof(err), out_candidates=ctypes.addressof(cand),
         out_launches=ctypes.addressof(launches), out_filter_error_bound=ctypes.addressof(bound),
     )

@@ -153,7 +153,8 @@ typedef struct hnsw_b200_exact_args {
     int32_t k;                     /* 1 <= k <= n */
     int32_t metric;                /* HNSW_B200_L2 / _IP / _COSINE */
     int32_t integer_valued;        /* 1: every data and query value is an integer with |v| <= 256
-                                      (exact in BF16: one tensor-core term instead of three) */
+                                      (exact in BF16: one tensor-core term instead of three); 0: not
+                                      known to be; -1: the library checks on the device */
     int32_t reserved;
     int64_t *out_ids;              /* (nq, k) int64, ascending (distance, id) */
     double *out_dists;             /* (nq, k) float64 exact distances */
