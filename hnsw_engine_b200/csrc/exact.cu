@@ -60,10 +60,7 @@ constexpr int CW = HB_EPI_CW;  // columns per TMEM load (16 or 32)
 static_assert(CW == 16 || CW == 32, "chunks of 16 or 32 columns");
 constexpr int EPI_PER_QUARTER = EPI_WARPS / 4;
 constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
-// Shared memory after the stage buffers: barriers and flags (BAR_BYTES), then every epilogue warp's
-// |x|^2 staging for its chunks of a tile (XW floats: at most ceil(BN / CW / parts) chunks of CW).
-constexpr int BAR_BYTES = 256;
-constexpr int XW = ((BN / CW + EPI_PER_QUARTER - 1) / EPI_PER_QUARTER) * CW;
+constexpr int BAR_BYTES = 256;  // barriers and flags after the stage buffers
 // Rows of at least COOP_DIM dimensions are re-scored by the whole warp, one candidate at a time.
 constexpr int COOP_DIM = 256;
 constexpr uint32_t TMEM_COLS = 512;  // two accumulators of BN columns
@@ -360,22 +357,9 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         int cnt = 0;  // this thread's appends (its own segment: no atomics)
         const bool l2 = p.metric == HNSW_B200_L2;
         const bool cosine = p.metric == HNSW_B200_COSINE;
-        // |x|^2 of this warp's chunks of the current tile (XW floats of shared memory per warp),
-        // loaded before the warp waits for the tile's accumulator, so their latency overlaps it.
-        float *xw = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES + BAR_BYTES) + (warp - 4) * XW;
-        const int my_chunks = (BN / CW - part + EPI_PER_QUARTER - 1) / EPI_PER_QUARTER;
         for (int lt = 0; lt < ntiles; lt++) {
             const int b = lt & 1;
             const int row0 = p.row_begin + (t0 + lt) * BN;
-            if (l2) {
-                if (lane < my_chunks * (CW / 4)) {  // xx holds n_pad >= row0 + BN entries
-                    const int ch = lane / (CW / 4), qd = lane % (CW / 4);
-                    const int col = (part + ch * EPI_PER_QUARTER) * CW + qd * 4;
-                    reinterpret_cast<float4 *>(xw)[lane] =
-                        __ldg(reinterpret_cast<const float4 *>(p.xx + row0 + col));
-                }
-                __syncwarp();
-            }
             int ok = 1;
             if (lane == 0) ok = mbar_wait(tfull + b, (lt >> 1) & 1, abort_flag) ? 1 : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -388,15 +372,18 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-            for (int c = part * CW, ch = 0; c < BN; c += CW * EPI_PER_QUARTER, ch++) {
+            for (int c = part * CW; c < BN; c += CW * EPI_PER_QUARTER) {
                 const int col0 = row0 + c;
-                // |x|^2 of the CW columns from this warp's staging (shared-memory broadcasts).
+                // |x|^2 of the CW columns: the same addresses in every lane (broadcast loads),
+                // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + CW
+                // entries (zero beyond the data rows). Staging them in shared memory per warp
+                // before the accumulator wait measured no faster (504 against 490 us).
                 float xv[CW];
                 if (l2) {
-                    const float4 *x4 = reinterpret_cast<const float4 *>(xw + ch * CW);
+                    const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
 #pragma unroll
                     for (int i = 0; i < CW / 4; i++) {
-                        const float4 t = x4[i];
+                        const float4 t = __ldg(x4 + i);
                         xv[4 * i] = t.x;
                         xv[4 * i + 1] = t.y;
                         xv[4 * i + 2] = t.z;
@@ -529,6 +516,81 @@ __device__ __forceinline__ uint32_t fkey(float f) {
 }
 __device__ __forceinline__ float funkey(uint32_t k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Bin of the rank-th key (1-based) from a block's 256-bin histogram, 256 threads: a warp scan,
+// then the 8 warp totals; exactly one thread writes the bucket and the rank within it.
+__device__ __forceinline__ void find_bucket(const uint32_t *hist, uint32_t *wsum, uint32_t rank,
+                                            uint32_t *s_bucket, uint32_t *s_rank) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t c = hist[threadIdx.x];
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    for (int w = 0; w < warp; w++) incl += wsum[w];
+    const uint32_t excl = incl - c;
+    if (excl < rank && rank <= incl) {
+        *s_bucket = uint32_t(threadIdx.x);
+        *s_rank = rank - excl;
+    }
+    __syncthreads();
+}
+
+// select_kth for long candidate lists (the prefix pass): one block of 256 threads per query, a
+// warp per segment.
+__global__ void select_kth_block(const float *cand_val, const int32_t *cand_cnt, int32_t cap,
+                                 int32_t nseg, int32_t nq, int32_t k, const float *margin,
+                                 float *out_thr, float *out_tau) {
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t wsum[8];
+    __shared__ uint32_t s_bucket, s_rank;
+    __shared__ int s_m;
+    const int q = blockIdx.x;
+    if (q >= nq) return;
+    const int wid = threadIdx.x >> 5, lid = threadIdx.x & 31;
+    const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
+    if (threadIdx.x == 0) s_m = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int sg = threadIdx.x; sg < nseg; sg += blockDim.x) mine += min(cnt[sg], cap);
+    atomicAdd(&s_m, mine);
+    __syncthreads();
+    const float *v = cand_val + int64_t(q) * nseg * cap;
+    if (s_m < k) {
+        if (threadIdx.x == 0) {
+            out_tau[q] = INFINITY;
+            out_thr[q] = INFINITY;
+        }
+        return;
+    }
+    uint32_t prefix = 0, rank = uint32_t(k);
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        hist[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t hmask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
+        for (int sg = wid; sg < nseg; sg += int(blockDim.x >> 5)) {
+            const int ms = min(cnt[sg], cap);
+            for (int i = lid; i < ms; i += 32) {
+                const uint32_t key = fkey(v[int64_t(sg) * cap + i]);
+                if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+            }
+        }
+        __syncthreads();
+        find_bucket(hist, wsum, rank, &s_bucket, &s_rank);
+        prefix |= s_bucket << shift;
+        rank = s_rank;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float tau = funkey(prefix);
+        out_tau[q] = tau;
+        out_thr[q] = tau + margin[q];
+    }
 }
 
 // One warp per query, 8 per block: tau[q] = k-th smallest of the candidate values (or +inf if
@@ -1021,7 +1083,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     CUtensorMap tmA, tmB;
     if (int rc = make_map(&tmA, qb, q_pad, kp, BM)) return rc;
     if (int rc = make_map(&tmB, xb, n_pad, kp, BN)) return rc;
-    const size_t smem = STAGES * STAGE_BYTES + 1024 + BAR_BYTES + size_t(EPI_WARPS) * XW * 4;
+    const size_t smem = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
     XT(cudaFuncSetAttribute(knn_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int wpb = 4;
     const size_t rsm = size_t(wpb) * (k + 1) * 12;
@@ -1075,8 +1137,9 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         XT(cudaMemcpyAsync(th, inf.data(), size_t(nq) * 4, cudaMemcpyHostToDevice, s));
         // One candidate per CW-row block suffices while the prefix has at least k blocks.
         if (int rc = run_filter(prefix, block_min)) return rc;
-        select_kth<<<int((nq + SELECT_WARPS - 1) / SELECT_WARPS), 32 * SELECT_WARPS, 0, s>>>(
-            cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg, th, tau);
+        // The prefix pass leaves long lists (a block per query); pass two short ones (a warp).
+        select_kth_block<<<int(nq), 256, 0, s>>>(cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq),
+                                                 k, mg, th, tau);
         // Pass two: every row against tau + margin.
         if (int rc = run_filter(n, false)) return rc;
         XT(cudaMemsetAsync(cstat, 0, 16, s));
