@@ -213,12 +213,14 @@ __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15)
 __host__ __device__ inline int result_slots(int ef_cap) { return ef_cap + 33; }
 
 // Shared memory of one warp: results, query (f64, f32 and bytes), filtered candidates, rerank top-k.
-// two_ids: the graph is stored in an internal node order, so results keep internal ids next to
-// the original ones (otherwise the two are the same array).
+// two_ids: the graph is stored in an internal node order, so filtered results and candidates keep
+// internal ids next to the original ones (otherwise, and always for unfiltered searches, whose
+// results hold internal ids only, the two are the same array).
 __host__ __device__ inline size_t warp_smem_bytes(int ef_cap, int dim, bool filtered, int s_cap,
                                                   int k_rerank, bool two_ids, int stage = 0) {
     size_t b = al16(size_t(stage)) + al16(size_t(result_slots(ef_cap)) * 8) +
-               (two_ids ? 2 : 1) * al16(size_t(result_slots(ef_cap)) * 4) + al16(size_t(dim) * 8) +
+               (two_ids && filtered ? 2 : 1) * al16(size_t(result_slots(ef_cap)) * 4) +
+               al16(size_t(dim) * 8) +
                al16(size_t(dim) * 4) + al16(size_t(dim));
     if (filtered) b += al16(size_t(s_cap + 1) * 8) + (two_ids ? 2 : 1) * al16(size_t(s_cap + 1) * 4);
     if (k_rerank > 0) b += al16(size_t(k_rerank + 1) * 8) + al16(size_t(k_rerank + 1) * 4);
@@ -272,20 +274,26 @@ struct CtxT {
 using Ctx = CtxT<double>;  // filtered searches and the float64 modes
 
 // Node arrays may be stored in any order (internal ids, chosen for memory locality); results,
-// and ties between equal distances, use the original ids. Sentinel ids outside [0, n) map to
-// themselves.
+// and ties between equal distances, use the original ids. Unfiltered result lists hold internal
+// ids and look the original ones up only for equal distances and at output. Sentinel ids outside
+// [0, n) map to themselves.
 __device__ __forceinline__ int32_t orig_id(const SearchParams &P, int32_t i) {
-#ifdef HB_NO_ID_LOOKUP
-    return i;
-#else
     return (P.node_ids != nullptr && i >= 0 && i < P.n) ? __ldg(P.node_ids + i) : i;
-#endif
 }
 
 // (distance, id) order of two entries whose ids are comparable as they are.
 template <typename T>
 __device__ __forceinline__ bool pair_lt_raw(T da, int32_t ia, T db, int32_t ib) {
     return da < db || (da == db && ia < ib);
+}
+
+// (distance, original id) order of two entries held by internal id: the id lookups run only for
+// equal distances, so the unfiltered result list carries internal ids alone.
+template <typename T>
+__device__ __forceinline__ bool pair_lt_int(const SearchParams &P, T da, int32_t ia, T db,
+                                            int32_t ib) {
+    if (da != db) return da < db;
+    return orig_id(P, ia) < orig_id(P, ib);
 }
 
 
@@ -314,6 +322,28 @@ __device__ __forceinline__ int sorted_rank(const T *Ad, const int32_t *Ai, int m
     const int base = (chunks - 1) * step;  // the last chunk starting below holds the boundary
     const int i = base + lane;
     const bool in = lane < step && i < m && pair_lt_raw(Ad[i], Ai[i] & ID_MASK, d, id);
+    return base + __popc(__ballot_sync(FULL, in));
+}
+
+// sorted_rank over entries held by internal ids (ordered by distance, then original id).
+template <typename T>
+__device__ __forceinline__ int sorted_rank_int(const SearchParams &P, const T *Ad,
+                                               const int32_t *Ai, int m, T d, int32_t id,
+                                               int lane) {
+    if (m > 1024) {
+        int c = 0;
+        for (int i = lane; i < m; i += 32) c += pair_lt_int(P, Ad[i], Ai[i] & ID_MASK, d, id);
+        return __reduce_add_sync(FULL, c);
+    }
+    const int step = (m + 31) >> 5;
+    const int s = lane * step;
+    const bool below = s < m && pair_lt_int(P, Ad[s], Ai[s] & ID_MASK, d, id);
+    const uint32_t b = __ballot_sync(FULL, below);
+    const int chunks = __popc(b);
+    if (chunks == 0) return 0;
+    const int base = (chunks - 1) * step;
+    const int i = base + lane;
+    const bool in = lane < step && i < m && pair_lt_int(P, Ad[i], Ai[i] & ID_MASK, d, id);
     return base + __popc(__ballot_sync(FULL, in));
 }
 
@@ -982,7 +1012,7 @@ __device__ __forceinline__ bool stop_checkpoint(const SearchParams &P, Cx &C, St
 // final worst, pushed in descending (distance, id) order as the evictions would have pushed them.
 // churn (a stop feature) counts admissions that entered the first k at their insertion time.
 template <class Cx>
-__device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_t e, int32_t eo,
+__device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_t e,
                                             typename Cx::dist_t dj, uint32_t um, int ef, int &r,
                                             typename Cx::dist_t &W, int &scan, int &tn, int &churn) {
     using D = typename Cx::dist_t;
@@ -1001,23 +1031,35 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
             else b = m;
         }
         lo = a;
-        for (int i = a; i < r0 && C.Rd[i] == dj; i++) {  // equal distances: rank by id
-            n_eq++;
-            eq_lt += (C.Ri[i] & ID_MASK) < eo;
+        if (a < r0 && C.Rd[a] == dj) {  // equal distances (rare): rank by original id
+            const int32_t eo = orig_id(P, e);
+            for (int i = a; i < r0 && C.Rd[i] == dj; i++) {
+                n_eq++;
+                eq_lt += orig_id(P, C.Ri[i] & ID_MASK) < eo;
+            }
         }
     }
 #if HB_ADMIT_MASKS
     // One pass over the candidates: the ones below mine by (distance, id), and the earlier ones at
     // or below my distance, as lane masks.
-    uint32_t ltm = 0u, plem = 0u;
+    uint32_t ltm = 0u, plem = 0u, teq = 0u;  // teq: other candidates at my distance
     for (uint32_t m = cm; m;) {
         const int i = __ffs(m) - 1;
         m &= m - 1;
         const D di = __shfl_sync(FULL, dj, i);
-        const int32_t ii = __shfl_sync(FULL, eo, i);
         const uint32_t bit = 1u << i;
-        ltm |= (di < dj || (di == dj && ii < eo)) ? bit : 0u;
+        ltm |= di < dj ? bit : 0u;
+        teq |= (di == dj && i != lane) ? bit : 0u;
         plem |= (i < lane && di <= dj) ? bit : 0u;
+    }
+    if (__any_sync(FULL, teq != 0u)) {  // rare: equal distances order by original id
+        const int32_t eo = inc ? orig_id(P, e) : -1;
+        for (uint32_t m = cm; m;) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t oi = __shfl_sync(FULL, eo, i);
+            ltm |= ((teq >> i) & 1u) && oi < eo ? 1u << i : 0u;
+        }
     }
     const bool adm = inc && lo + n_eq + __popc(plem) < ef;
     const uint32_t A = __ballot_sync(FULL, adm);
@@ -1041,8 +1083,8 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
         const int i = __ffs(m) - 1;
         m &= m - 1;
         const D di = __shfl_sync(FULL, dj, i);
-        const int32_t ii = __shfl_sync(FULL, eo, i);
-        const bool lt = di < dj || (di == dj && ii < eo);
+        const int32_t ii = __shfl_sync(FULL, e, i);
+        const bool lt = di < dj || (di == dj && i != lane && pair_lt_int(P, di, ii, dj, e));
         rank_a += lt;
         rank_prev += (lt && i < lane);
     }
@@ -1059,16 +1101,14 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
         const int p1 = top - lane, p2 = top - 32 - lane;
         const bool a1 = p1 >= pmin, a2 = p2 >= pmin;
         D d1 = D(0), d2 = D(0);
-        int32_t i1 = 0, i2 = 0, q1 = 0, q2 = 0;
+        int32_t i1 = 0, i2 = 0;
         if (a1) {
             d1 = C.Rd[p1];
             i1 = C.Ri[p1];
-            q1 = C.Rp[p1];
         }
         if (a2) {
             d2 = C.Rd[p2];
             i2 = C.Ri[p2];
-            q2 = C.Rp[p2];
         }
         int s1 = 0, s2 = 0;
         for (uint32_t m = A; m;) {
@@ -1082,19 +1122,16 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
         if (a1) {
             C.Rd[p1 + s1] = d1;
             C.Ri[p1 + s1] = i1;
-            C.Rp[p1 + s1] = q1;
         }
         if (a2) {
             C.Rd[p2 + s2] = d2;
             C.Ri[p2 + s2] = i2;
-            C.Rp[p2 + s2] = q2;
         }
         __syncwarp();
     }
     if (adm) {
         C.Rd[fpos] = dj;
-        C.Ri[fpos] = eo;
-        C.Rp[fpos] = e;
+        C.Ri[fpos] = e;
     }
     __syncwarp();
     int rn = r0 + __popc(A);
@@ -1105,7 +1142,7 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
         bool push = false;
         int32_t pid = 0;
         if (lane < nev) {
-            pid = C.Rp[ef + lane] & ID_MASK;
+            pid = C.Ri[ef + lane] & ID_MASK;
             push = C.Rd[ef + lane] == wf && !(C.Ri[ef + lane] & EXP_BIT);
         }
         const uint32_t pm = __ballot_sync(FULL, push);
@@ -1130,11 +1167,11 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
     const int lane = C.lane;
     if (layer > 0 || (cfg_hash(CFG) && log2 > 0)) {
         vis_clear(C.vis, log2, lane);
-        if (lane == 0) vis_insert(C.vis, log2, C.Rp[0] & ID_MASK);
+        if (lane == 0) vis_insert(C.vis, log2, C.Ri[0] & ID_MASK);
         __syncwarp();
     } else {
         log2 = 0;  // bitmap
-        bitmap_begin(P, C, C.Rp[0] & ID_MASK);
+        bitmap_begin(P, C, C.Ri[0] & ID_MASK);
     }
     int vis_count = 1;
     const int vis_lim = log2 > 0 ? ((1 << log2) >> 2) * 3 : 0x7fffffff;
@@ -1153,8 +1190,8 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
             const uint32_t b = __ballot_sync(FULL, un);
             if (b) {
                 const int p = scan + __ffs(b) - 1;
-                c = C.Rp[p] & ID_MASK;
                 const int32_t co = C.Ri[p];
+                c = co & ID_MASK;
                 scan = p + 1;
                 __syncwarp();
                 if (lane == 0) C.Ri[p] = co | EXP_BIT;
@@ -1175,7 +1212,6 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
         const int32_t e0 = first_link(nb, stride, cnt, lane);
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? e0 : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
-            const int32_t eo = e >= 0 ? orig_id(P, e) : -1;  // needed only at admission
 #ifdef HB_PROFILE
             __syncwarp();
             if (__shfl_sync(FULL, e, 0) == -2) C.status |= 64;  // consume the load before timing
@@ -1190,7 +1226,7 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
             HB_PROF(5);
             C.ndist += __popc(um);
             if (layer == 0 && HB_BATCH_ADMIT) {
-                admit_chunk(P, C, e, eo, dj, um, ef, r, W, scan, tn, S.churn);
+                admit_chunk(P, C, e, dj, um, ef, r, W, scan, tn, S.churn);
                 HB_PROF(4);
                 continue;
             }
@@ -1199,15 +1235,13 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
                 const int j = __ffs(am) - 1;
                 am &= am - 1;
                 const D d = __shfl_sync(FULL, dj, j);
-                const int32_t id = __shfl_sync(FULL, eo, j);
-                const int32_t pid = __shfl_sync(FULL, e, j);
+                const int32_t id = __shfl_sync(FULL, e, j);
                 if (!(r < ef || d < W)) continue;  // uniform
-                const int pos = sorted_rank(C.Rd, C.Ri, r, d, id, lane);
-                shift_up(C.Rd, C.Ri, pos, r, lane, C.Rp != C.Ri ? C.Rp : nullptr);
+                const int pos = sorted_rank_int(P, C.Rd, C.Ri, r, d, id, lane);
+                shift_up(C.Rd, C.Ri, pos, r, lane);
                 if (lane == 0) {
                     C.Rd[pos] = d;
                     C.Ri[pos] = id;
-                    C.Rp[pos] = pid;
                 }
                 __syncwarp();
                 r++;
@@ -1220,7 +1254,7 @@ __device__ void layer_search(const SearchParams &P, Cx &C, int layer, int ef, in
                     if (ed == C.Rd[ef - 1]) {
                         if (!(ei & EXP_BIT)) {  // still a candidate, tied with the worst
                             if (tn < P.tie_cap) {
-                                if (lane == 0) C.ties[tn] = C.Rp[ef] & ID_MASK;
+                                if (lane == 0) C.ties[tn] = ei & ID_MASK;
                                 tn++;
                             } else {
                                 C.status |= ST_TIES;
@@ -1477,15 +1511,17 @@ __device__ void layer0_filtered(const SearchParams &P, Cx &C, int ef, int log2, 
 // ------------------------------------------------------------------------------ rerank epilogue
 // numba_engine._rerank_batch (:506-530): exact float64 distances from the float32 query to the
 // first m beam entries, best k by (distance, id).
+// internal: R holds internal ids only (unfiltered); otherwise Ri holds the original ids.
 template <class Cx>
-__device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m) {
+__device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m, bool internal) {
     const int lane = C.lane;
     const int k = P.k;
     int a = 0;
     for (int base = 0; base < m; base += 32) {
         const int i = base + lane;
         const bool has = i < m;
-        const int32_t id = has ? (C.Ri[i] & ID_MASK) : -1;  // original id
+        const int32_t ri = has ? (C.Ri[i] & ID_MASK) : -1;
+        const int32_t id = has && internal ? orig_id(P, ri) : ri;  // original id
         const double d = has ? dist_seq_f64<false>(P, C.Rp[i] & ID_MASK, C.qd) : INFINITY;
         uint32_t am = __ballot_sync(FULL, has);
         while (am) {
@@ -1515,7 +1551,7 @@ __global__ void __launch_bounds__(WPB * 32, min_blocks<MODE, FILT, CFG>())
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const bool rerank = P.rerank_queries != nullptr;
-    const bool two_ids = P.node_ids != nullptr;
+    const bool two_ids = P.node_ids != nullptr;  // filtered results keep both ids
     const int stage = stage_bytes(MODE, CFG, P.lane_rows, P.dim);
     const size_t wb = warp_smem_bytes(P.ef_cap, P.dim, FILT, P.s_cap, rerank ? P.k : 0, two_ids, stage);
     unsigned char *p = smem + size_t(warp) * wb;
@@ -1529,7 +1565,7 @@ __global__ void __launch_bounds__(WPB * 32, min_blocks<MODE, FILT, CFG>())
     C.Ri = reinterpret_cast<int32_t *>(p);
     p += al16(size_t(result_slots(P.ef_cap)) * 4);
     C.Rp = C.Ri;  // same ids: one array (reads of Rp mask the expanded bit)
-    if (two_ids) {
+    if (two_ids && FILT) {
         C.Rp = reinterpret_cast<int32_t *>(p);
         p += al16(size_t(result_slots(P.ef_cap)) * 4);
     }
@@ -1618,34 +1654,31 @@ __global__ void __launch_bounds__(WPB * 32, min_blocks<MODE, FILT, CFG>())
             C.qfeat = log1pf(float(ss));
         }
         // Entry point, then greedy descent (ef = 1) through the upper layers.
+        // layer_search keeps internal ids in Ri (ties order by original id through lookups).
         int32_t e0 = int32_t(P.entry_point);  // internal id
-        int32_t o0 = orig_id(P, e0);            // original id
         double d0 = dist_one<MODE, U8>(P, C, e0);
         C.ndist++;
         int r = 1;
         for (int layer = P.max_level; layer > 0 && !C.status; layer--) {
             if (lane == 0) {
                 C.Rd[0] = D(d0);
-                C.Ri[0] = o0;
-                C.Rp[0] = e0;
+                C.Ri[0] = e0;
             }
             __syncwarp();
             r = 1;
             layer_search<MODE, U8, CFG>(P, C, layer, 1, P.vis_up_log2, r);
             d0 = C.Rd[0];
-            o0 = C.Ri[0] & ID_MASK;
-            e0 = C.Rp[0] & ID_MASK;
+            e0 = C.Ri[0] & ID_MASK;
             __syncwarp();
         }
         const int ef0 = max(__ldg(P.ef + q), P.k_search);
         if (!C.status) {
             if constexpr (FILT) {
-                layer0_filtered<MODE, U8, CFG>(P, C, ef0, P.vis_log2, d0, e0, o0, r);
+                layer0_filtered<MODE, U8, CFG>(P, C, ef0, P.vis_log2, d0, e0, orig_id(P, e0), r);
             } else {
                 if (lane == 0) {
                     C.Rd[0] = D(d0);
-                    C.Ri[0] = o0;
-                    C.Rp[0] = e0;
+                    C.Ri[0] = e0;
                 }
                 __syncwarp();
                 r = 1;
@@ -1668,14 +1701,15 @@ __global__ void __launch_bounds__(WPB * 32, min_blocks<MODE, FILT, CFG>())
             const float *rq = P.rerank_queries + int64_t(q) * dim;
             for (int i = lane; i < dim; i += 32) C.qd[i] = double(rq[i]);
             __syncwarp();
-            const int a = rerank_epilogue(P, C, min(r, P.k_search));
+            const int a = rerank_epilogue(P, C, min(r, P.k_search), !FILT);
             for (int i = lane; i < k; i += 32) {
                 oi[i] = i < a ? int64_t(C.Ai[i]) : -1;
                 od[i] = i < a ? C.Ad[i] : INFINITY;
             }
         } else {
             for (int i = lane; i < k; i += 32) {
-                oi[i] = i < r ? int64_t(C.Ri[i] & ID_MASK) : -1;
+                const int32_t ri = i < r ? (C.Ri[i] & ID_MASK) : -1;
+                oi[i] = i < r ? int64_t(FILT ? ri : orig_id(P, ri)) : -1;
                 od[i] = i < r ? double(C.Rd[i]) : double(INFINITY);
             }
         }
