@@ -71,6 +71,15 @@ constexpr uint32_t IDESC = (1u << 4)            // c_format F32
                            | (1u << 7)          // a_format BF16
                            | (1u << 10)         // b_format BF16
                            | (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+// The same for byte rows (kind::i8): unsigned 8-bit A and B (formats 0), S32 accumulator (c_format
+// 2). Integer products and sums are exact, so the filter values are the exact distances.
+constexpr uint32_t IDESC_I8 = (2u << 4) | (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+// Byte rows: a K chunk of one stage is 128 elements (one 128-byte swizzle row), 32 per instruction.
+constexpr int BK8 = 128;
+// Largest |distance| whose float value is exact (integers below 2^24).
+constexpr float EXACT_LIM = 16777216.f;
+// Filter value of a padding column in the byte path: above every distance the path admits.
+constexpr int32_t I8_PAD = 0x3fffffff;
 
 struct FilterParams {
     int32_t nq;            // valid queries
@@ -81,6 +90,8 @@ struct FilterParams {
     int32_t metric;
     const float *qq;       // |q|^2 per query (l2)
     const float *xx;       // |x|^2 per row (l2)
+    const int32_t *qqi;    // byte rows: exact |q|^2 per query (l2)
+    const int32_t *xxi;    // byte rows: exact |x|^2 per row (l2)
     const float *thr;      // per query: tau + margin (+inf in pass one)
     // Candidates in segments: every epilogue thread of the grid owns one segment of its query's
     // list (segment = row split x epilogue part), so appends need no atomics. Segment s of query q
@@ -133,13 +144,17 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
 }
 
 // Bounded wait: false if the wall-clock limit expired (the caller records the error).
+// The abort flag and the clock are read every 64th probe: a waiting thread then issues little
+// besides the probes, leaving the issue slots to the warps that work.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = now_ns();
-    for (;;) {
+    for (uint32_t i = 1;; i++) {
         if (mbar_try(bar, parity)) return true;
-        if (*abort_flag) return false;
-        if (now_ns() - t0 > WAIT_LIMIT_NS) return false;
+        if ((i & 63u) == 0u) {
+            if (*abort_flag) return false;
+            if (now_ns() - t0 > WAIT_LIMIT_NS) return false;
+        }
     }
 }
 
@@ -171,6 +186,16 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
         "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_u8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(IDESC_I8), "r"(accumulate)
         : "memory");
 }
 
@@ -217,6 +242,8 @@ __device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[W]) {
     else tmem_ld32(taddr, v);
 }
 
+// I8: byte rows on kind::i8 (exact integer filter values); otherwise BF16 terms on kind::f16.
+template <bool I8>
 __global__ void __launch_bounds__(FILTER_THREADS, 1)
     knn_filter_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const FilterParams p) {
@@ -279,8 +306,8 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 unsigned char *a = smem + s * STAGE_BYTES;
                 unsigned char *b = a + A_BYTES;
                 mbar_expect_tx(full + s, STAGE_BYTES);
-                tma_load_2d(&tmA, full + s, a, kc * BK, qt * BM);
-                tma_load_2d(&tmB, full + s, b, kc * BK, row0);
+                tma_load_2d(&tmA, full + s, a, kc * (I8 ? BK8 : BK), qt * BM);
+                tma_load_2d(&tmB, full + s, b, kc * (I8 ? BK8 : BK), row0);
             }
         }
         if (!ok) {
@@ -318,9 +345,13 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
                 const uint32_t b_addr = a_addr + A_BYTES;
 #pragma unroll
-                for (int j = 0; j < BK / 16; j++) {  // K = 16 per instruction, 32 bytes apart
-                    umma_bf16(tmem_d, sw128_desc(a_addr + j * 32), sw128_desc(b_addr + j * 32),
-                              (kc | j) != 0);
+                for (int j = 0; j < 4; j++) {  // 32 bytes of K per instruction (16 BF16 or 32 bytes)
+                    if constexpr (I8)
+                        umma_u8(tmem_d, sw128_desc(a_addr + j * 32), sw128_desc(b_addr + j * 32),
+                                (kc | j) != 0);
+                    else
+                        umma_bf16(tmem_d, sw128_desc(a_addr + j * 32), sw128_desc(b_addr + j * 32),
+                                  (kc | j) != 0);
                 }
                 umma_commit(empty + s);
             }
@@ -348,7 +379,8 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
         const int row = quarter * 32 + lane;  // TMEM lane = query row of the tile
         const int q = qt * BM + row;
         const bool qvalid = q < p.nq;
-        const float qq = qvalid ? p.qq[q] : 0.f;
+        const float qq = (qvalid && !I8) ? p.qq[q] : 0.f;
+        const int32_t qqi = (qvalid && I8) ? p.qqi[q] : 0;
         const float thr = qvalid ? p.thr[q] : -INFINITY;
         const int nseg = int(gridDim.y) * EPI_PER_QUARTER;
         const int64_t seg = int64_t(qvalid ? q : 0) * nseg + int64_t(blockIdx.y) * EPI_PER_QUARTER + part;
@@ -371,53 +403,91 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // TMEM columns of this warp's lane quarter in accumulator b
+            const uint32_t tbase = tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN);
 #pragma unroll 1
             for (int c = part * CW; c < BN; c += CW * EPI_PER_QUARTER) {
                 const int col0 = row0 + c;
-                // |x|^2 of the CW columns: the same addresses in every lane (broadcast loads),
-                // issued before the TMEM load so both latencies overlap. xx holds n_pad >= col0 + CW
-                // entries (zero beyond the data rows). Staging them in shared memory per warp
-                // before the accumulator wait measured no faster (504 against 490 us).
-                float xv[CW];
-                if (l2) {
-                    const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
-#pragma unroll
-                    for (int i = 0; i < CW / 4; i++) {
-                        const float4 t = __ldg(x4 + i);
-                        xv[4 * i] = t.x;
-                        xv[4 * i + 1] = t.y;
-                        xv[4 * i + 2] = t.z;
-                        xv[4 * i + 3] = t.w;
-                    }
-                }
-                float v[CW];
-                tmem_ld<CW>(tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN + c), v);
                 const int valid = min(CW, p.row_end - col0);  // columns that are data rows
                 // The filter value is a = v + vadd with v = |x|^2 - 2 q.x (l2), -q.x (ip, cosine)
-                // and vadd = |q|^2, 0, 1: one FMA or negation per element, then the chunk's
-                // minimum. fl(v + vadd) is monotonic in v, so a chunk whose minimum fails the
-                // threshold has no candidate; the rare chunks with one test each element.
-                if (l2) {
+                // and vadd = |q|^2, 0, 1: one FMA (integer multiply-add) or negation per element,
+                // then the chunk's minimum. a is monotonic in v (float rounding included), so a
+                // chunk whose minimum fails the threshold has no candidate; the rare chunks with
+                // one test each element. |x|^2 of the CW columns is loaded with the same addresses
+                // in every lane (broadcast loads), before the TMEM load so both latencies overlap;
+                // the |x|^2 arrays hold n_pad >= col0 + CW entries (zero beyond the data rows).
+                // Staging them in shared memory per warp measured no faster (504 against 490 us).
+                float v[CW];     // BF16 path: v; byte path: the raw S32 accumulator bits
+                int32_t w[CW];   // byte path: v, exact
+                float amin, vadd = 0.f;
+                int32_t vaddi = 0;
+                if constexpr (I8) {
+                    int32_t xv[CW];
+                    if (l2) {
+                        const int4 *x4 = reinterpret_cast<const int4 *>(p.xxi + col0);
 #pragma unroll
-                    for (int j = 0; j < CW; j++) v[j] = fmaf(-2.f, v[j], xv[j]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < CW; j++) v[j] = -v[j];
-                }
-                if (valid < CW) {  // uniform: only the last tile of the rows
+                        for (int i = 0; i < CW / 4; i++) {
+                            const int4 t = __ldg(x4 + i);
+                            xv[4 * i] = t.x;
+                            xv[4 * i + 1] = t.y;
+                            xv[4 * i + 2] = t.z;
+                            xv[4 * i + 3] = t.w;
+                        }
+                    }
+                    tmem_ld<CW>(tbase + uint32_t(c), v);
 #pragma unroll
                     for (int j = 0; j < CW; j++)
-                        if (j >= valid) v[j] = INFINITY;
+                        w[j] = l2 ? xv[j] - 2 * __float_as_int(v[j]) : -__float_as_int(v[j]);
+                    if (valid < CW) {  // uniform: only the last tile of the rows
+#pragma unroll
+                        for (int j = 0; j < CW; j++)
+                            if (j >= valid) w[j] = I8_PAD;
+                    }
+                    int32_t mh[CW / 2];
+#pragma unroll
+                    for (int j = 0; j < CW / 2; j++) mh[j] = min(w[j], w[j + CW / 2]);
+#pragma unroll
+                    for (int s2 = CW / 4; s2 > 0; s2 >>= 1)
+#pragma unroll
+                        for (int j = 0; j < s2; j++) mh[j] = min(mh[j], mh[j + s2]);
+                    vaddi = l2 ? qqi : 0;
+                    amin = float(mh[0] + vaddi);
+                } else {
+                    float xv[CW];
+                    if (l2) {
+                        const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
+#pragma unroll
+                        for (int i = 0; i < CW / 4; i++) {
+                            const float4 t = __ldg(x4 + i);
+                            xv[4 * i] = t.x;
+                            xv[4 * i + 1] = t.y;
+                            xv[4 * i + 2] = t.z;
+                            xv[4 * i + 3] = t.w;
+                        }
+                    }
+                    tmem_ld<CW>(tbase + uint32_t(c), v);
+                    if (l2) {
+#pragma unroll
+                        for (int j = 0; j < CW; j++) v[j] = fmaf(-2.f, v[j], xv[j]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < CW; j++) v[j] = -v[j];
+                    }
+                    if (valid < CW) {  // uniform: only the last tile of the rows
+#pragma unroll
+                        for (int j = 0; j < CW; j++)
+                            if (j >= valid) v[j] = INFINITY;
+                    }
+                    float mh[CW / 2];
+#pragma unroll
+                    for (int j = 0; j < CW / 2; j++) mh[j] = fminf(v[j], v[j + CW / 2]);
+#pragma unroll
+                    for (int s2 = CW / 4; s2 > 0; s2 >>= 1)
+#pragma unroll
+                        for (int j = 0; j < s2; j++) mh[j] = fminf(mh[j], mh[j + s2]);
+                    vadd = l2 ? qq : (cosine ? 1.f : 0.f);
+                    amin = mh[0] + vadd;
                 }
-                float mh[CW / 2];
-#pragma unroll
-                for (int j = 0; j < CW / 2; j++) mh[j] = fminf(v[j], v[j + CW / 2]);
-#pragma unroll
-                for (int w = CW / 4; w > 0; w >>= 1)
-#pragma unroll
-                    for (int j = 0; j < w; j++) mh[j] = fminf(mh[j], mh[j + w]);
-                const float vadd = l2 ? qq : (cosine ? 1.f : 0.f);
-                const float amin = mh[0] + vadd;
                 if (p.block_min) {
                     // Threshold pass: the k-th smallest of the blocks' minima is at least the k-th
                     // smallest of all the values (a subset's k-th is never below the set's), so
@@ -432,7 +502,7 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 } else if (qvalid && amin <= thr) {
 #pragma unroll
                     for (int j = 0; j < CW; j++) {  // static indices keep v[] in registers
-                        const float a = v[j] + vadd;
+                        const float a = I8 ? float(w[j] + vaddi) : v[j] + vadd;
                         if (j < valid && a <= thr) {
                             if (cnt < p.cap) {
                                 cv[cnt] = a;
@@ -458,6 +528,34 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------------- prep
+// Byte rows (values checked to be integers in [0, 255]): one warp per row writes the u8 operand row
+// of width kpad (a multiple of 128, zero past dim), four bytes a lane, and the exact |x|^2.
+template <typename T>
+__global__ void prep_rows_u8(const T *src, int64_t rows, int dim, int64_t rows_pad, int kpad,
+                             uint8_t *dst, int32_t *sq) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wpb = blockDim.x >> 5;
+    for (int64_t r = int64_t(blockIdx.x) * wpb + (threadIdx.x >> 5); r < rows_pad;
+         r += int64_t(gridDim.x) * wpb) {
+        uint32_t *out = reinterpret_cast<uint32_t *>(dst + r * kpad);
+        const T *x = src + r * dim;
+        int32_t ss = 0;
+        for (int i = lane * 4; i < kpad; i += 128) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int32_t v = (r < rows && i + t < dim) ? int32_t(x[i + t]) : 0;
+                ss += v * v;
+                word |= uint32_t(v & 255) << (8 * t);
+            }
+            out[i >> 2] = word;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        if (lane == 0) sq[r] = ss;
+    }
+}
+
 // One warp per row: float64 norm, cosine normalisation, BF16 operand row(s) of width kpad.
 // terms == 1: [v]; terms == 3: A-side [hi, hi, lo] (queries) or B-side [hi, lo, hi] (data).
 template <typename T>
@@ -672,14 +770,62 @@ __device__ __forceinline__ bool pair_lt(double da, int32_t ia, double db, int32_
     return da < db || (da == db && ia < ib);
 }
 
+// Float64 distance of row x to the query qv by one lane, the sums in dimension order.
+template <typename T>
+__device__ __forceinline__ double dist_f64_lane(const T *x, const T *qv, int dim, int metric,
+                                                double xn, double qn) {
+    double acc = 0.0;
+    if (metric == HNSW_B200_L2) {
+        for (int j = 0; j < dim; j++) {
+            const double df = __dsub_rn(double(x[j]), double(qv[j]));
+            acc = __dadd_rn(acc, __dmul_rn(df, df));
+        }
+        return acc;
+    }
+    if (metric == HNSW_B200_IP) {
+        for (int j = 0; j < dim; j++) acc = __dadd_rn(acc, __dmul_rn(double(x[j]), double(qv[j])));
+        return -acc;
+    }
+    for (int j = 0; j < dim; j++)
+        acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[j]), xn), __ddiv_rn(double(qv[j]), qn)));
+    return __dsub_rn(1.0, acc);
+}
+
+// The same by the whole warp (long rows): lane l sums dimensions l, l + 32, ..., then a fixed
+// shuffle tree adds the lanes (the same value on every run; on integer data every order gives the
+// same exact sum), so the float64 chains are 32 times shorter. The result is on every lane.
+template <typename T>
+__device__ __forceinline__ double dist_f64_warp(const T *x, const T *qv, int dim, int metric,
+                                                double xn, double qn, int lane) {
+    double acc = 0.0;
+    if (metric == HNSW_B200_L2) {
+        for (int i = lane; i < dim; i += 32) {
+            const double df = __dsub_rn(double(x[i]), double(qv[i]));
+            acc = __dadd_rn(acc, __dmul_rn(df, df));
+        }
+    } else if (metric == HNSW_B200_IP) {
+        for (int i = lane; i < dim; i += 32) acc = __dadd_rn(acc, __dmul_rn(double(x[i]), double(qv[i])));
+    } else {
+        for (int i = lane; i < dim; i += 32)
+            acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[i]), xn), __ddiv_rn(double(qv[i]), qn)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+    return metric == HNSW_B200_L2 ? acc : (metric == HNSW_B200_IP ? -acc : __dsub_rn(1.0, acc));
+}
+
 // One warp per query: exact float64 distances of the candidates within the final threshold,
 // best k by (distance, id) kept in shared memory (sorted insertion), written as int64 / float64.
+// exact_lim > 0 (byte rows, integer filter): a candidate whose filter value is below exact_lim in
+// magnitude already holds its exact distance and is not re-scored; the k results are re-scored in
+// float64 at the end instead, and any difference sets *mismatch.
 template <typename T>
 __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq, int32_t k,
                             int32_t metric, const double *xnorm, const double *qnorm,
                             const float *cand_val, const int32_t *cand_id, const int32_t *cand_cnt,
                             int32_t cap, int32_t nseg, const float *thr, int64_t *out_ids,
-                            double *out_d, unsigned long long *err_max) {
+                            double *out_d, unsigned long long *err_max, float exact_lim,
+                            int32_t *mismatch) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int warps = blockDim.x >> 5;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -690,9 +836,10 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
     if (q >= nq) return;
     const float t = thr[q];
     const T *qv = queries + int64_t(q) * dim;
-    const double qn = qnorm[q];
+    const bool cos = metric == HNSW_B200_COSINE;
+    const double qn = cos ? qnorm[q] : 1.0;
     int a = 0;
-    double err = 0.0;  // largest |filter value - exact distance| over this lane's survivors
+    double err = 0.0;  // largest |filter value - exact distance| over this lane's re-scored survivors
     // Batches of 32 candidates taken across the segments in order, so every lane scores one
     // (segments hold a few entries each).
     const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
@@ -714,59 +861,23 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
             }
         }
         const float approx = at >= 0 ? cand_val[at] : INFINITY;
-        bool has = at >= 0 && approx <= t;
-        int32_t id = has ? cand_id[at] : -1;
-        double d = INFINITY;
+        const bool has = at >= 0 && approx <= t;
+        const int32_t id = has ? cand_id[at] : -1;
+        const bool known = has && fabsf(approx) < exact_lim;  // exact already (byte rows)
+        const bool need = has && !known;
+        double d = known ? double(approx) : INFINITY;
         if (dim >= COOP_DIM) {
-            // Long rows: the warp scores the batch's candidates one after another, each lane
-            // summing every 32nd dimension and a fixed shuffle tree adding the lanes (the same value
-            // on every run; on integer data every order gives the same exact sum), so the float64
-            // chains are 32 times shorter than one lane per candidate.
-            for (uint32_t hm = __ballot_sync(0xffffffffu, has); hm; hm &= hm - 1) {
+            for (uint32_t hm = __ballot_sync(0xffffffffu, need); hm; hm &= hm - 1) {
                 const int j = __ffs(hm) - 1;
                 const int32_t idj = __shfl_sync(0xffffffffu, id, j);
-                const T *x = data + int64_t(idj) * dim;
-                double acc = 0.0;
-                if (metric == HNSW_B200_L2) {
-                    for (int i = lane; i < dim; i += 32) {
-                        const double df = __dsub_rn(double(x[i]), double(qv[i]));
-                        acc = __dadd_rn(acc, __dmul_rn(df, df));
-                    }
-                } else if (metric == HNSW_B200_IP) {
-                    for (int i = lane; i < dim; i += 32)
-                        acc = __dadd_rn(acc, __dmul_rn(double(x[i]), double(qv[i])));
-                } else {
-                    const double xn = xnorm[idj];
-                    for (int i = lane; i < dim; i += 32)
-                        acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[i]), xn),
-                                                       __ddiv_rn(double(qv[i]), qn)));
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, o));
-                if (lane == j)
-                    d = metric == HNSW_B200_L2 ? acc : (metric == HNSW_B200_IP ? -acc : __dsub_rn(1.0, acc));
+                const double dd = dist_f64_warp(data + int64_t(idj) * dim, qv, dim, metric,
+                                                cos ? xnorm[idj] : 1.0, qn, lane);
+                if (lane == j) d = dd;
             }
-            if (has) err = fmax(err, fabs(double(approx) - d));
-        } else if (has) {
-            const T *x = data + int64_t(id) * dim;
-            double acc = 0.0;
-            if (metric == HNSW_B200_L2) {
-                for (int j = 0; j < dim; j++) {
-                    const double df = __dsub_rn(double(x[j]), double(qv[j]));
-                    acc = __dadd_rn(acc, __dmul_rn(df, df));
-                }
-                d = acc;
-            } else if (metric == HNSW_B200_IP) {
-                for (int j = 0; j < dim; j++) acc = __dadd_rn(acc, __dmul_rn(double(x[j]), double(qv[j])));
-                d = -acc;
-            } else {
-                const double xn = xnorm[id];
-                for (int j = 0; j < dim; j++)
-                    acc = __dadd_rn(acc, __dmul_rn(__ddiv_rn(double(x[j]), xn), __ddiv_rn(double(qv[j]), qn)));
-                d = __dsub_rn(1.0, acc);
-            }
-            err = fmax(err, fabs(double(approx) - d));
+        } else if (need) {
+            d = dist_f64_lane(data + int64_t(id) * dim, qv, dim, metric, cos ? xnorm[id] : 1.0, qn);
         }
+        if (need) err = fmax(err, fabs(double(approx) - d));
         uint32_t am = __ballot_sync(0xffffffffu, has);
         while (am) {
             const int j = __ffs(am) - 1;
@@ -800,6 +911,19 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
             a = min(a + 1, k);
         }
     }
+    if (exact_lim > 0.f) {  // the results taken from filter values, re-scored in float64
+        bool bad = false;
+        if (dim >= COOP_DIM) {
+            for (int r = 0; r < a; r++) {
+                const double dd = dist_f64_warp(data + int64_t(Ai[r]) * dim, qv, dim, metric, 1.0, qn, lane);
+                bad |= dd != Ad[r];
+            }
+        } else {
+            for (int r = lane; r < a; r += 32)
+                bad |= dist_f64_lane(data + int64_t(Ai[r]) * dim, qv, dim, metric, 1.0, qn) != Ad[r];
+        }
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(mismatch, 1);
+    }
     for (int r = lane; r < k; r += 32) {
         out_ids[int64_t(q) * k + r] = r < a ? int64_t(Ai[r]) : -1;
         out_d[int64_t(q) * k + r] = r < a ? Ad[r] : INFINITY;
@@ -812,15 +936,22 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
     if (lane == 0 && eb) atomicMax(err_max, eb);
 }
 
-// Whether every value is an integer with |v| <= 256 (exact in BF16): *flag gets 1 when one is not.
+// Value classes of a float array: *flag gets bit 1 when a value is not an integer with |v| <= 256
+// (exact in BF16), bit 2 when one is not an integer in [0, 255] (a byte). Written with explicit
+// branches and an integer OR across the warp: a form that combined two boolean warp votes set the
+// wrong bits on the GPU (every non-integer and 300 read as bytes), this one was checked against
+// those values there.
 __global__ void check_small_int(const float *x, int64_t count, int32_t *flag) {
-    bool bad = false;
+    int f = 0;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
          i += int64_t(gridDim.x) * blockDim.x) {
         const float v = x[i];
-        bad |= !(v == rintf(v) && fabsf(v) <= 256.f);
+        const float r = rintf(v);
+        if (r != v || !(fabsf(v) <= 256.f)) f |= 1;
+        if (r != v || !(v >= 0.f) || !(v <= 255.f)) f |= 2;
     }
-    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+    f = int(__reduce_or_sync(0xffffffffu, uint32_t(f)));
+    if (f && (threadIdx.x & 31) == 0) atomicOr(flag, f);
 }
 
 // Largest and total of the segment counts (overflow check and the candidate total).
@@ -886,14 +1017,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-int make_map(CUtensorMap *map, const void *base, int64_t rows, int kpad, int box_rows) {
+// Tiled map of a row-major operand of kpad elements a row: boxes of one 128-byte swizzle row (BK
+// BF16 or BK8 bytes) by box_rows rows.
+int make_map(CUtensorMap *map, const void *base, int64_t rows, int kpad, int box_rows, bool u8 = false) {
     auto fn = encode_fn();
     if (!fn) return fail(HNSW_B200_ECUDA, "cuTensorMapEncodeTiled unavailable");
     cuuint64_t dims[2] = {cuuint64_t(kpad), cuuint64_t(rows)};
-    cuuint64_t strides[1] = {cuuint64_t(kpad) * 2};
-    cuuint32_t box[2] = {cuuint32_t(BK), cuuint32_t(box_rows)};
+    cuuint64_t strides[1] = {cuuint64_t(kpad) * (u8 ? 1 : 2)};
+    cuuint32_t box[2] = {cuuint32_t(u8 ? BK8 : BK), cuuint32_t(box_rows)};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+    CUresult r = fn(map, u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                    const_cast<void *>(base), dims, strides,
                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(HNSW_B200_ECUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(int(r)));
@@ -938,6 +1072,12 @@ constexpr int64_t CAND_BYTES = int64_t(4) << 30;
 #define HB_EXPECT_FACTOR 2
 #endif
 constexpr int64_t EXPECT_FACTOR = HB_EXPECT_FACTOR;
+// Byte rows use the integer filter (1) or the BF16 one (0).
+#ifndef HB_EXACT_I8
+#define HB_EXACT_I8 1
+#endif
+// Longest byte row of the integer filter: 2 dim 255^2 stays below 2^31.
+constexpr int MAX_DIM_I8 = 8192;
 // Prefix length. Pass one costs the prefix's rows on the tensor cores; pass two then keeps about
 // k n / prefix rows per query, each re-scored in float64 (and a per-element epilogue path on the
 // chunks holding them). A float64 re-score of a row costs about PREFIX_BALANCE times a row of
@@ -955,25 +1095,31 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     const int64_t n = a->n, nq_all = a->nq;
     const int dim = a->dim, k = a->k, metric = a->metric;
     int integer = a->integer_valued;
-    if (integer < 0) {  // find out on the device: bytes always are; floats by one pass each
+    // Byte rows (every value an integer in [0, 255], L2 or inner product, int32-safe sums) take the
+    // integer tensor-core filter, whose values are the exact distances.
+    const bool bytes_ok = HB_EXACT_I8 && metric != HNSW_B200_COSINE && dim <= MAX_DIM_I8;
+    bool bytes = false;
+    if constexpr (std::is_same_v<T, uint8_t>) {
         integer = 1;
-        if constexpr (std::is_same_v<T, float>) {
-            static thread_local Scratch flag_buf;
-            if (int rc = flag_buf.get(16)) return rc;
-            int32_t *flag = static_cast<int32_t *>(flag_buf.p);
-            XT(cudaMemsetAsync(flag, 0, 4, s));
-            check_small_int<<<1024, 256, 0, s>>>(static_cast<const float *>(a->data), n * dim, flag);
-            check_small_int<<<256, 256, 0, s>>>(static_cast<const float *>(a->queries), nq_all * dim, flag);
-            XT(cudaGetLastError());
-            int32_t hflag = 0;
-            XT(cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s));
-            XT(cudaStreamSynchronize(s));
-            integer = hflag ? 0 : 1;
-        }
+        bytes = bytes_ok;
+    } else if (integer != 0) {  // find out on the device, one pass over each array
+        static thread_local Scratch flag_buf;
+        if (int rc = flag_buf.get(16)) return rc;
+        int32_t *flag = static_cast<int32_t *>(flag_buf.p);
+        XT(cudaMemsetAsync(flag, 0, 4, s));
+        check_small_int<<<1024, 256, 0, s>>>(static_cast<const float *>(a->data), n * dim, flag);
+        check_small_int<<<256, 256, 0, s>>>(static_cast<const float *>(a->queries), nq_all * dim, flag);
+        XT(cudaGetLastError());
+        int32_t hflag = 0;
+        XT(cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s));
+        XT(cudaStreamSynchronize(s));
+        if (integer < 0) integer = (hflag & 1) ? 0 : 1;
+        bytes = bytes_ok && (hflag & 3) == 0;
     }
     const int terms = integer && metric != HNSW_B200_COSINE ? 1 : 3;
     const int seg = (dim + BK - 1) / BK * BK;
-    const int kp = seg * terms;
+    // K of a row: BF16 elements (terms segments), or bytes in 128-byte chunks
+    const int kp = bytes ? (dim + BK8 - 1) / BK8 * BK8 : seg * terms;
     const int64_t n_pad = (n + BN - 1) / BN * BN;
     int sms = 148;
     int dev = 0;
@@ -1029,8 +1175,9 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         off += al256(bytes);
         return o;
     };
-    const size_t o_xb = carve(size_t(n_pad) * kp * 2);
-    const size_t o_qb = carve(size_t(q_pad) * kp * 2);
+    const size_t esz = bytes ? 1 : 2;  // operand element bytes
+    const size_t o_xb = carve(size_t(n_pad) * kp * esz);
+    const size_t o_qb = carve(size_t(q_pad) * kp * esz);
     const size_t o_xn = carve(size_t(n_pad) * 8);
     const size_t o_qn = carve(size_t(q_pad) * 8);
     const size_t o_xx = carve(size_t(n_pad) * 4);
@@ -1053,6 +1200,10 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     auto *qn = reinterpret_cast<double *>(B + o_qn);
     auto *xx = reinterpret_cast<float *>(B + o_xx);
     auto *qq = reinterpret_cast<float *>(B + o_qq);
+    auto *xb8 = reinterpret_cast<uint8_t *>(B + o_xb);  // byte path: the same buffers as u8 / int32
+    auto *qb8 = reinterpret_cast<uint8_t *>(B + o_qb);
+    auto *xxi = reinterpret_cast<int32_t *>(B + o_xx);
+    auto *qqi = reinterpret_cast<int32_t *>(B + o_qq);
     auto *mg = reinterpret_cast<float *>(B + o_mg);
     auto *th = reinterpret_cast<float *>(B + o_th);
     auto *tau = reinterpret_cast<float *>(B + o_tau);
@@ -1064,12 +1215,16 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     const int cos = metric == HNSW_B200_COSINE;
     int64_t launches = 0;
 
-    prep_rows<T><<<int(std::min<int64_t>(4096, (n_pad + 7) / 8)), 256, 0, s>>>(
-        X, n, dim, n_pad, kp, terms, 0, cos, xb, xn, xx);
+    if (bytes)
+        prep_rows_u8<T><<<int(std::min<int64_t>(4096, (n_pad + 7) / 8)), 256, 0, s>>>(
+            X, n, dim, n_pad, kp, xb8, xxi);
+    else
+        prep_rows<T><<<int(std::min<int64_t>(4096, (n_pad + 7) / 8)), 256, 0, s>>>(
+            X, n, dim, n_pad, kp, terms, 0, cos, xb, xn, xx);
     XT(cudaGetLastError());
     launches++;
     double xmax = 1.0;  // largest data norm (margins): a device reduction, one 8-byte copy
-    if (!cos) {
+    if (!cos && !bytes) {
         auto *mx = reinterpret_cast<unsigned long long *>(B + o_mx);
         XT(cudaMemsetAsync(mx, 0, 8, s));
         max_norm_kernel<<<int(std::min<int64_t>(1024, (n + 255) / 256)), 256, 0, s>>>(xn, n, mx);
@@ -1081,10 +1236,11 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         launches++;
     }
     CUtensorMap tmA, tmB;
-    if (int rc = make_map(&tmA, qb, q_pad, kp, BM)) return rc;
-    if (int rc = make_map(&tmB, xb, n_pad, kp, BN)) return rc;
+    if (int rc = make_map(&tmA, B + o_qb, q_pad, kp, BM, bytes)) return rc;
+    if (int rc = make_map(&tmB, B + o_xb, n_pad, kp, BN, bytes)) return rc;
     const size_t smem = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
-    XT(cudaFuncSetAttribute(knn_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    XT(cudaFuncSetAttribute(knn_filter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    XT(cudaFuncSetAttribute(knn_filter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int wpb = 4;
     const size_t rsm = size_t(wpb) * (k + 1) * 12;
     if (rsm > 200 * 1024) return fail(HNSW_B200_EINVAL, "k too large for the rerank kernel");
@@ -1100,9 +1256,15 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     for (int64_t q0 = 0; q0 < nq_all; q0 += QB) {
         const int64_t nq = std::min<int64_t>(QB, nq_all - q0);
         const T *Q = static_cast<const T *>(a->queries) + q0 * dim;
-        prep_rows<T><<<int(std::min<int64_t>(4096, (q_pad + 7) / 8)), 256, 0, s>>>(
-            Q, nq, dim, q_pad, kp, terms, 1, cos, qb, qn, qq);
-        margins_kernel<<<int((nq + 255) / 256), 256, 0, s>>>(qn, int32_t(nq), xmax, kp, terms, metric, mg);
+        if (bytes) {  // exact filter values: no margin
+            prep_rows_u8<T><<<int(std::min<int64_t>(4096, (q_pad + 7) / 8)), 256, 0, s>>>(
+                Q, nq, dim, q_pad, kp, qb8, qqi);
+            XT(cudaMemsetAsync(mg, 0, size_t(nq) * 4, s));
+        } else {
+            prep_rows<T><<<int(std::min<int64_t>(4096, (q_pad + 7) / 8)), 256, 0, s>>>(
+                Q, nq, dim, q_pad, kp, terms, 1, cos, qb, qn, qq);
+            margins_kernel<<<int((nq + 255) / 256), 256, 0, s>>>(qn, int32_t(nq), xmax, kp, terms, metric, mg);
+        }
         XT(cudaGetLastError());
         launches += 2;
         // Query tiles of this chunk only (the last chunk may be short), rows split to fill the GPU.
@@ -1116,11 +1278,13 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
             fp.nq = int32_t(nq);
             fp.row_begin = 0;
             fp.row_end = int32_t(row_end);
-            fp.kchunks = kp / BK;
+            fp.kchunks = kp / (bytes ? BK8 : BK);
             fp.tiles_per_split = tps;
             fp.metric = metric;
             fp.qq = qq;
             fp.xx = xx;
+            fp.qqi = qqi;
+            fp.xxi = xxi;
             fp.thr = th;
             fp.cand_val = cv;
             fp.cand_id = ci;
@@ -1128,7 +1292,10 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
             fp.cap = int32_t(cap);
             fp.block_min = bmin ? 1 : 0;
             fp.err = err;
-            knn_filter_kernel<<<dim3(qt_chunk, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
+            if (bytes)
+                knn_filter_kernel<true><<<dim3(qt_chunk, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
+            else
+                knn_filter_kernel<false><<<dim3(qt_chunk, splits), FILTER_THREADS, smem, s>>>(tmA, tmB, fp);
             XT(cudaGetLastError());
             launches++;
             return 0;
@@ -1165,15 +1332,34 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
             cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg, th, tau);
         rerank_topk<T><<<int((nq + wpb - 1) / wpb), wpb * 32, rsm, s>>>(
             X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), int32_t(nseg), th,
-            a->out_ids + q0 * k, a->out_dists + q0 * k, ferr);
+            a->out_ids + q0 * k, a->out_dists + q0 * k, ferr, bytes ? EXACT_LIM : 0.f, err + 1);
         XT(cudaGetLastError());
         launches += 3;
         if (a->out_filter_error_bound) {
+            // BF16 filter: half the largest margin. Byte rows: the integer distances are exact and
+            // only their float copies of 2^24 or more round, by at most half a float ulp of the
+            // final threshold (counted here as a margin of a whole ulp).
             std::vector<float> hm(static_cast<size_t>(nq));
-            XT(cudaMemcpyAsync(hm.data(), mg, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
+            XT(cudaMemcpyAsync(hm.data(), bytes ? th : mg, size_t(nq) * 4, cudaMemcpyDeviceToHost, s));
             XT(cudaStreamSynchronize(s));
-            for (float v : hm) max_margin = std::max(max_margin, double(v));
+            for (float v : hm) {
+                // inner product: candidates reach below the threshold, down to -dim 255^2
+                if (bytes && metric == HNSW_B200_IP) v = float(dim) * 65025.f;
+                if (!bytes) {
+                    max_margin = std::max(max_margin, double(v));
+                } else if (std::fabs(v) >= EXACT_LIM && std::isfinite(v)) {
+                    int e = 0;
+                    std::frexp(double(std::fabs(v)), &e);  // |v| in [2^(e-1), 2^e)
+                    max_margin = std::max(max_margin, std::ldexp(1.0, e - 24));
+                }
+            }
         }
+    }
+    if (bytes) {  // the integer results against their float64 re-scores
+        int32_t hm[4];
+        XT(cudaMemcpyAsync(hm, err, 16, cudaMemcpyDeviceToHost, s));
+        XT(cudaStreamSynchronize(s));
+        if (hm[1]) return fail(HNSW_B200_ECUDA, "exact knn: an integer filter distance differs from its float64 re-score");
     }
     if (a->out_filter_error_bound) *a->out_filter_error_bound = max_margin / 2.0;
     if (a->out_filter_max_error) {

@@ -3,8 +3,11 @@
 ``exact_search(data, queries, k, metric)`` keeps the reference's signature and result contract
 (``src/hnsw_engine/oracle.py:35-126``): ``(ids int64 (nq, k), distances float64 (nq, k))`` sorted
 by ascending distance with ties broken by ascending id. The work runs in ``libhnsw_b200``
-(``hnsw_b200_exact_knn``): a BF16 tensor-core distance filter with FP32 accumulation and a
-derived error margin, then a float64 re-rank of the survivors.
+(``hnsw_b200_exact_knn``): a tensor-core distance filter, then the k best survivors by
+(distance, id). Byte rows (uint8, or float32 rows of integers in [0, 255]) under L2 or inner
+product take the integer filter (tcgen05 kind::i8), whose values are the exact distances; other
+rows take a BF16 filter with FP32 accumulation and a derived error margin, and their survivors are
+re-ranked in float64.
 """
 
 from __future__ import annotations

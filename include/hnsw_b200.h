@@ -154,21 +154,28 @@ typedef struct hnsw_b200_exact_args {
     int32_t metric;                /* HNSW_B200_L2 / _IP / _COSINE */
     int32_t integer_valued;        /* 1: every data and query value is an integer with |v| <= 256
                                       (exact in BF16: one tensor-core term instead of three); 0: not
-                                      known to be; -1: the library checks on the device */
+                                      known to be; -1: the library checks on the device. Float rows
+                                      are checked on the device for bytes unless this is 0 */
     int32_t reserved;
     int64_t *out_ids;              /* (nq, k) int64, ascending (distance, id) */
     double *out_dists;             /* (nq, k) float64 exact distances */
     double *out_filter_max_error;  /* host: largest |filter value - float64 distance| measured over
-                                      every re-scored candidate of the call, or NULL */
+                                      every re-scored candidate of the call, or NULL (byte rows:
+                                      only candidates whose float value is 2^24 or more are
+                                      re-scored, and the k results are checked in float64) */
     int64_t *out_candidates;       /* host: candidates re-scored in float64, or NULL */
     int64_t *out_launches;         /* host: kernel launches made, or NULL */
     double *out_filter_error_bound; /* host: largest derived bound e_q of the filter's error (the
                                       margin is 2 e_q), or NULL; the measured error never exceeds it */
 } hnsw_b200_exact_args_t;
 
-/* Exact k nearest neighbours by brute force on the tensor cores (BF16 filter with FP32
- * accumulation and a derived error margin, then float64 re-rank of the survivors, ties to the
- * lower id). Replaces oracle.exact_search (src/hnsw_engine/oracle.py:35-126). Synchronises
+/* Exact k nearest neighbours by brute force on the tensor cores, ties to the lower id. Byte rows
+ * (u8, or float rows whose every value is an integer in [0, 255]; L2 or inner product; dim <= 8192)
+ * take an integer filter (tcgen05 kind::i8, S32 accumulation) whose values are the exact
+ * distances, so no margin is needed and only float copies of 2^24 or more are re-scored; a float64
+ * re-score of the k results that differs from them fails the call (HNSW_B200_ECUDA). Other rows
+ * take a BF16 filter with FP32 accumulation and a derived error margin, then a float64 re-rank of
+ * the survivors. Replaces oracle.exact_search (src/hnsw_engine/oracle.py:35-126). Synchronises
  * `stream`. When more rows fall within a query's margin than its candidate list holds (many exact
  * ties at the k-th distance), the call re-runs with longer lists (fewer queries per chunk) instead
  * of failing. */

@@ -71,6 +71,54 @@ def test_image_like_uint8_matches_oracle(metric: str) -> None:
     np.testing.assert_array_equal(u8[0], o_ids)
 
 
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_byte_rows_of_any_width_match_oracle(metric: str) -> None:
+    """The integer filter (byte rows) at widths around its 128-byte K chunks, values at both ends
+    of [0, 255] and inner products beyond 2^24 (dim 1000): ids and distances bit-exact, and the
+    measured error (float copies of 2^24 or more only) within the bound."""
+    from hnsw_engine_b200.exact_knn import exact_search
+    from oracle import exact
+
+    rng = np.random.default_rng(21)
+    for dim in (1, 127, 129, 1000):
+        data = rng.integers(0, 256, (3000, dim)).astype(np.float32)
+        data[:50] = 255.0
+        data[50:100] = 0.0
+        queries = rng.integers(0, 256, (40, dim)).astype(np.float32)
+        queries[0] = 255.0
+        queries[1] = 0.0
+        ids, dists, st = exact_search(data, queries, 20, metric, return_stats=True)
+        o_ids, o_d = exact.exact_search(data, queries, 20, metric)
+        np.testing.assert_array_equal(ids, o_ids, err_msg=f"dim {dim}")
+        np.testing.assert_array_equal(dists, o_d, err_msg=f"dim {dim}")
+        assert 0.0 <= st.filter_max_error <= st.filter_error_bound
+        u8 = exact_search(data.astype(np.uint8), queries.astype(np.uint8), 20, metric)
+        np.testing.assert_array_equal(u8[0], o_ids)
+        np.testing.assert_array_equal(u8[1], o_d)
+
+
+def test_integer_rows_outside_bytes_and_cosine_bytes_match_oracle() -> None:
+    """Signed integer rows (not bytes: the BF16 filter, one term) and byte rows under cosine (also
+    the BF16 filter) against the oracle."""
+    from hnsw_engine_b200.exact_knn import exact_search
+    from oracle import exact
+
+    rng = np.random.default_rng(22)
+    data = rng.integers(-128, 128, (5000, 64)).astype(np.float32)
+    queries = rng.integers(-128, 128, (30, 64)).astype(np.float32)
+    for metric in ("l2", "ip"):
+        ids, dists, st = exact_search(data, queries, 15, metric, return_stats=True)
+        o_ids, o_d = exact.exact_search(data, queries, 15, metric)
+        np.testing.assert_array_equal(ids, o_ids, err_msg=metric)
+        np.testing.assert_array_equal(dists, o_d, err_msg=metric)
+        assert st.filter_error_bound > 0.0  # signed values: the BF16 filter with its margins
+    b = rng.integers(0, 256, (5000, 64)).astype(np.uint8)
+    qb = rng.integers(0, 256, (30, 64)).astype(np.uint8)
+    ids, dists = exact_search(b, qb, 15, "cosine")
+    o_ids, o_d = exact.exact_search(b, qb, 15, "cosine")
+    assert_same_neighbors(ids, dists, o_ids, o_d, atol=1e-12)
+
+
 @pytest.mark.parametrize("metric", ["l2", "ip", "cosine"])
 def test_float_data_matches_oracle(metric: str) -> None:
     from hnsw_engine_b200.exact_knn import exact_search
@@ -79,9 +127,11 @@ def test_float_data_matches_oracle(metric: str) -> None:
     rng = np.random.default_rng(3)
     data = rng.standard_t(3.0, (20000, 100)).astype(np.float32)
     queries = rng.standard_t(3.0, (50, 100)).astype(np.float32)
-    ids, dists = exact_search(data, queries, 10, metric)
+    ids, dists, st = exact_search(data, queries, 10, metric, return_stats=True)
     o_ids, o_d = exact.exact_search(data, queries, 10, metric)
     assert_same_neighbors(ids, dists, o_ids, o_d, atol=1e-9 if metric != "cosine" else 1e-12)
+    assert st.filter_error_bound > 0.0  # not bytes: the BF16 filter with its margins
+    assert 0.0 <= st.filter_max_error <= st.filter_error_bound
 
 
 def test_mixture_1m_shape_subset_matches_oracle() -> None:
@@ -106,7 +156,7 @@ def _sample_rows(nq: int, count: int) -> np.ndarray:
 def test_full_mixture_config_1m_x_128_k100_matches_oracle() -> None:
     """The 1M x 128 mixture with its 10K queries at k = 100, searched in full on the GPU; a spread
     sample of 256 queries against the CPU restatement of oracle.exact_search over all 1M rows.
-    Integer data at d = 128: the filter arithmetic is exact, so the measured error is 0."""
+    Byte rows at d = 128 (distances below 2^24): the filter values are exact, error and bound 0."""
     from hnsw_engine_b200 import synthetic
     from hnsw_engine_b200.exact_knn import exact_search
     from oracle import exact
@@ -119,13 +169,14 @@ def test_full_mixture_config_1m_x_128_k100_matches_oracle() -> None:
     np.testing.assert_array_equal(ids[rows], o_ids)
     np.testing.assert_array_equal(dists[rows], o_d)
     assert st.filter_max_error == 0.0
-    assert st.filter_max_error <= st.filter_error_bound
+    assert st.filter_error_bound == 0.0
 
 
 def test_full_image_config_60k_x_784_k100_matches_oracle() -> None:
     """The 60K x 784 image-like uint8 set with its 10K queries at k = 100 on the GPU; a spread
-    sample of 256 queries against the CPU oracle, ids and distances bit-exact. Sums reach beyond
-    2^24 here, so the filter is approximate: its measured error must stay within the bound."""
+    sample of 256 queries against the CPU oracle, ids and distances bit-exact. Byte rows take the
+    integer filter: its distances are exact, and only float copies of 2^24 or more may round, within
+    the bound."""
     from hnsw_engine_b200 import synthetic
     from hnsw_engine_b200.exact_knn import exact_search
     from oracle import exact
