@@ -691,22 +691,72 @@ __global__ void select_kth_block(const float *cand_val, const int32_t *cand_cnt,
     }
 }
 
+// Moves one query's candidates (segments of `cap` entries, counts in cnt) to the front of its
+// region, in segment order, by one warp; returns how many there are. In place: an entry's new index
+// (its rank in segment order) is never above its old one, and the warp moves the entries in rank
+// order, 32 at a time, reading a batch before writing it, so no entry is overwritten before it has
+// moved. A lane finds its entry's segment by a binary search over the 32 segment offsets of the
+// group (shuffles).
+__device__ __forceinline__ int compact_list(float *v, int32_t *id, const int32_t *cnt, int32_t cap,
+                                            int32_t nseg, int lane) {
+    int base = 0;
+    for (int s0 = 0; s0 < nseg; s0 += 32) {
+        const int sg = s0 + lane;
+        const int n_sg = sg < nseg ? min(cnt[sg], cap) : 0;
+        int incl = n_sg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - n_sg;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int b = 0; b < total; b += 32) {
+            const int r = b + lane;  // rank within the group
+            int lo = 0;  // last segment of the group whose offset is <= r (every lane searches)
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int e = __shfl_sync(0xffffffffu, excl, min(lo + step, 31));
+                if (lo + step < 32 && e <= r) lo += step;
+            }
+            const int off = __shfl_sync(0xffffffffu, excl, lo);
+            float val = 0.f;
+            int32_t ident = 0;
+            if (r < total) {
+                const int64_t src = int64_t(s0 + lo) * cap + (r - off);
+                val = v[src];
+                ident = id[src];
+            }
+            __syncwarp();
+            if (r < total) {
+                v[base + r] = val;
+                id[base + r] = ident;
+            }
+            __syncwarp();
+        }
+        base += total;
+    }
+    return base;
+}
+
 // One warp per query, 8 per block: tau[q] = k-th smallest of the candidate values (or +inf if
 // fewer than k), then out_thr[q] = tau + margin[q]. A 4-pass radix select, 8 bits a pass, over the
 // query's segments; the bin of the rank-th key comes from each lane's 8 bins and a warp scan.
 constexpr int SELECT_WARPS = 8;
-__global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32_t cap, int32_t nseg,
-                           int32_t nq, int32_t k, const float *margin, float *out_thr, float *out_tau) {
+// The query's list is first compacted in place (compact_list) and its length stored in
+// cand_m[q], so the radix passes and the re-rank read one dense run of entries.
+__global__ void select_kth(float *cand_val, int32_t *cand_id, const int32_t *cand_cnt, int32_t cap,
+                           int32_t nseg, int32_t nq, int32_t k, const float *margin, float *out_thr,
+                           float *out_tau, int32_t *cand_m) {
     __shared__ uint32_t hist_all[SELECT_WARPS][256];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = blockIdx.x * SELECT_WARPS + wid;
     if (q >= nq) return;  // no block-wide barrier below
     uint32_t *hist = hist_all[wid];
-    const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
-    int m = 0;
-    for (int sg = lane; sg < nseg; sg += 32) m += min(cnt[sg], cap);
-    m = __reduce_add_sync(0xffffffffu, m);
-    const float *v = cand_val + int64_t(q) * nseg * cap;
+    float *v = cand_val + int64_t(q) * nseg * cap;
+    const int m = compact_list(v, cand_id + int64_t(q) * nseg * cap, cand_cnt + int64_t(q) * nseg,
+                               cap, nseg, lane);
+    if (lane == 0) cand_m[q] = m;
     if (m < k) {
         if (lane == 0) {
             out_tau[q] = INFINITY;
@@ -719,12 +769,9 @@ __global__ void select_kth(const float *cand_val, const int32_t *cand_cnt, int32
         for (int i = lane; i < 256; i += 32) hist[i] = 0;
         __syncwarp();
         const uint32_t hmask = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
-        for (int sg = 0; sg < nseg; sg++) {
-            const int ms = min(cnt[sg], cap);
-            for (int i = lane; i < ms; i += 32) {
-                const uint32_t key = fkey(v[int64_t(sg) * cap + i]);
-                if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
-            }
+        for (int i = lane; i < m; i += 32) {
+            const uint32_t key = fkey(v[i]);
+            if ((key & hmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
         }
         __syncwarp();
         uint32_t c[8], sum = 0;
@@ -822,7 +869,7 @@ __device__ __forceinline__ double dist_f64_warp(const T *x, const T *qv, int dim
 template <typename T>
 __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq, int32_t k,
                             int32_t metric, const double *xnorm, const double *qnorm,
-                            const float *cand_val, const int32_t *cand_id, const int32_t *cand_cnt,
+                            const float *cand_val, const int32_t *cand_id, const int32_t *cand_m,
                             int32_t cap, int32_t nseg, const float *thr, int64_t *out_ids,
                             double *out_d, unsigned long long *err_max, float exact_lim,
                             int32_t *mismatch) {
@@ -840,26 +887,12 @@ __global__ void rerank_topk(const T *data, const T *queries, int dim, int32_t nq
     const double qn = cos ? qnorm[q] : 1.0;
     int a = 0;
     double err = 0.0;  // largest |filter value - exact distance| over this lane's re-scored survivors
-    // Batches of 32 candidates taken across the segments in order, so every lane scores one
-    // (segments hold a few entries each).
-    const int32_t *cnt = cand_cnt + int64_t(q) * nseg;
-    int sg = 0, off = 0;
-    while (sg < nseg && min(cnt[sg], cap) == 0) sg++;
-    while (sg < nseg) {
-        int64_t at = -1;  // this lane's entry
-        int filled = 0;
-        while (filled < 32 && sg < nseg) {  // uniform
-            const int c = min(cnt[sg], cap);
-            const int take = min(c - off, 32 - filled);
-            if (lane >= filled && lane < filled + take) at = (int64_t(q) * nseg + sg) * cap + off + (lane - filled);
-            filled += take;
-            off += take;
-            if (off >= c) {
-                off = 0;
-                sg++;
-                while (sg < nseg && min(cnt[sg], cap) == 0) sg++;
-            }
-        }
+    // The query's candidates, compacted by select_kth to the front of its region: batches of 32,
+    // one per lane.
+    const int m = cand_m[q];
+    const int64_t region = int64_t(q) * nseg * cap;
+    for (int b0 = 0; b0 < m; b0 += 32) {
+        const int64_t at = b0 + lane < m ? region + b0 + lane : -1;  // this lane's entry
         const float approx = at >= 0 ? cand_val[at] : INFINITY;
         const bool has = at >= 0 && approx <= t;
         const int32_t id = has ? cand_id[at] : -1;
@@ -1186,6 +1219,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     const size_t o_th = carve(size_t(QB) * 4);
     const size_t o_tau = carve(size_t(QB) * 4);
     const size_t o_cnt = carve(size_t(slots) * 4);
+    const size_t o_cm = carve(size_t(QB) * 4);
     const size_t o_cv = carve(size_t(slots) * cap * 4);
     const size_t o_ci = carve(size_t(slots) * cap * 4);
     const size_t o_cs = carve(16);
@@ -1208,6 +1242,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     auto *th = reinterpret_cast<float *>(B + o_th);
     auto *tau = reinterpret_cast<float *>(B + o_tau);
     auto *cnt = reinterpret_cast<int32_t *>(B + o_cnt);
+    auto *cm = reinterpret_cast<int32_t *>(B + o_cm);  // per query: candidates after compaction
     auto *cv = reinterpret_cast<float *>(B + o_cv);
     auto *ci = reinterpret_cast<int32_t *>(B + o_ci);
     auto *err = reinterpret_cast<int32_t *>(B + o_err);
@@ -1329,9 +1364,9 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
         }
         // The k-th smallest candidate is the global k-th approximate distance: final threshold.
         select_kth<<<int((nq + SELECT_WARPS - 1) / SELECT_WARPS), 32 * SELECT_WARPS, 0, s>>>(
-            cv, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg, th, tau);
+            cv, ci, cnt, int32_t(cap), int32_t(nseg), int32_t(nq), k, mg, th, tau, cm);
         rerank_topk<T><<<int((nq + wpb - 1) / wpb), wpb * 32, rsm, s>>>(
-            X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cnt, int32_t(cap), int32_t(nseg), th,
+            X, Q, dim, int32_t(nq), k, metric, xn, qn, cv, ci, cm, int32_t(cap), int32_t(nseg), th,
             a->out_ids + q0 * k, a->out_dists + q0 * k, ferr, bytes ? EXACT_LIM : 0.f, err + 1);
         XT(cudaGetLastError());
         launches += 3;
