@@ -162,7 +162,8 @@ typedef struct hnsw_b200_exact_args {
     double *out_filter_max_error;  /* host: largest |filter value - float64 distance| measured over
                                       every re-scored candidate of the call, or NULL (byte rows:
                                       only candidates whose float value is 2^24 or more are
-                                      re-scored, and the k results are checked in float64) */
+                                      re-scored, and one result in 16 of each query is checked in
+                                      float64) */
     int64_t *out_candidates;       /* host: candidates re-scored in float64, or NULL */
     int64_t *out_launches;         /* host: kernel launches made, or NULL */
     double *out_filter_error_bound; /* host: largest derived bound e_q of the filter's error (the
@@ -173,7 +174,8 @@ typedef struct hnsw_b200_exact_args {
  * (u8, or float rows whose every value is an integer in [0, 255]; L2 or inner product; dim <= 8192)
  * take an integer filter (tcgen05 kind::i8, S32 accumulation) whose values are the exact
  * distances, so no margin is needed and only float copies of 2^24 or more are re-scored; a float64
- * re-score of the k results that differs from them fails the call (HNSW_B200_ECUDA). Other rows
+ * re-score of one result in 16 of each query that differs from it fails the call
+ * (HNSW_B200_ECUDA). Other rows
  * take a BF16 filter with FP32 accumulation and a derived error margin, then a float64 re-rank of
  * the survivors. Replaces oracle.exact_search (src/hnsw_engine/oracle.py:35-126). Synchronises
  * `stream`. When more rows fall within a query's margin than its candidate list holds (many exact
