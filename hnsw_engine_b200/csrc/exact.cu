@@ -60,7 +60,8 @@ constexpr int CW = HB_EPI_CW;  // columns per TMEM load (16 or 32)
 static_assert(CW == 16 || CW == 32, "chunks of 16 or 32 columns");
 constexpr int EPI_PER_QUARTER = EPI_WARPS / 4;
 constexpr int FILTER_THREADS = 128 + 32 * EPI_WARPS;
-constexpr int BAR_BYTES = 256;  // barriers and flags after the stage buffers
+constexpr int BAR_BYTES = 256;  // barriers and flags after the stage buffers and the |x|^2 ring
+constexpr int XSLOTS = 4;       // |x|^2 ring slots (one tile's BN values each)
 // Rows of at least COOP_DIM dimensions are re-scored by the whole warp, one candidate at a time.
 constexpr int COOP_DIM = 256;
 // Byte rows: one result in VERIFY_EVERY of each query is re-scored in float64 as a check.
@@ -169,6 +170,16 @@ __device__ __forceinline__ void tma_load_2d(const CUtensorMap *map, uint64_t *ba
         : "memory");
 }
 
+// Plain (untiled, non-multicast) bulk copy of `bytes` from this GPU's global memory into shared
+// memory, completing on bar: both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // Shared-memory matrix descriptor, K-major, 128-byte swizzle: rows of 128 bytes, 8-row groups
 // 1024 bytes apart (stride byte offset), leading byte offset 16 bytes, descriptor version 1.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -253,11 +264,16 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
     // 1024-byte aligned stage buffers (swizzle-128B atoms), barriers after them.
     unsigned char *smem = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    // |x|^2 of a tile's BN rows (float or int32, 4 bytes each) in a ring of XSLOTS, after the
+    // stages: the producer fills slot lt % XSLOTS, the epilogue reads it and releases it.
+    unsigned char *xring = smem + STAGES * STAGE_BYTES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(xring + XSLOTS * BN * 4);
     uint64_t *empty = full + STAGES;
     uint64_t *tfull = empty + STAGES;
     uint64_t *tempty = tfull + 2;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tempty + 2);
+    uint64_t *xfull = tempty + 2;
+    uint64_t *xempty = xfull + XSLOTS;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(xempty + XSLOTS);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
@@ -277,6 +293,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             mbar_init(tfull + b, 1);
             mbar_init(tempty + b, EPI_WARPS);
         }
+        for (int x = 0; x < XSLOTS; x++) {
+            mbar_init(xfull + x, 1);
+            mbar_init(xempty + x, EPI_WARPS);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -294,10 +314,22 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
 
     if (warp == 0 && lane == 0) {
         // ---------------------------------------------------------------- TMA producer
-        int it = 0;
+        int it = 0, xs = 0;  // stages and |x|^2 slots issued
         bool ok = true;
         for (int lt = 0; lt < ntiles && ok; lt++) {
             const int row0 = p.row_begin + (t0 + lt) * BN;
+            {  // the tile's |x|^2 (rows row0 .. row0 + BN - 1 < n_pad) into its ring slot
+                const int x = lt % XSLOTS;
+                if (!mbar_wait(xempty + x, ((lt / XSLOTS) & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(xfull + x, BN * 4);
+                const void *src = I8 ? static_cast<const void *>(p.xxi + row0)
+                                     : static_cast<const void *>(p.xx + row0);
+                bulk_load(xring + x * BN * 4, src, BN * 4, xfull + x);
+                xs++;
+            }
             for (int kc = 0; kc < p.kchunks; kc++, it++) {
                 const int s = it % STAGES;
                 const uint32_t par = ((it / STAGES) & 1) ^ 1;
@@ -316,13 +348,20 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             atomicExch(p.err, 1);
             *abort_flag = 1;
         }
-        // Drain: every stage issued must land before the CTA may exit.
+        // Drain: every stage and |x|^2 slot issued must land before the CTA may exit.
         const int issued = it;
         for (int j = max(0, issued - STAGES); j < issued; j++) {
             const int s = j % STAGES;
             const uint32_t par = (j / STAGES) & 1;
             const unsigned long long t = now_ns();
             while (!mbar_try(full + s, par) && now_ns() - t < WAIT_LIMIT_NS) {
+            }
+        }
+        for (int j = max(0, xs - XSLOTS); j < xs; j++) {
+            const int x = j % XSLOTS;
+            const uint32_t par = (j / XSLOTS) & 1;
+            const unsigned long long t = now_ns();
+            while (!mbar_try(xfull + x, par) && now_ns() - t < WAIT_LIMIT_NS) {
             }
         }
     } else if (warp == 1 && lane == 0) {
@@ -395,7 +434,11 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             const int b = lt & 1;
             const int row0 = p.row_begin + (t0 + lt) * BN;
             int ok = 1;
-            if (lane == 0) ok = mbar_wait(tfull + b, (lt >> 1) & 1, abort_flag) ? 1 : 0;
+            if (lane == 0)
+                ok = (mbar_wait(tfull + b, (lt >> 1) & 1, abort_flag) &&
+                      mbar_wait(xfull + lt % XSLOTS, (lt / XSLOTS) & 1, abort_flag))
+                         ? 1
+                         : 0;
             ok = __shfl_sync(0xffffffffu, ok, 0);
             if (!ok) {
                 if (lane == 0) {
@@ -405,8 +448,9 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // TMEM columns of this warp's lane quarter in accumulator b
+            // TMEM columns of this warp's lane quarter in accumulator b; the tile's |x|^2 in its slot
             const uint32_t tbase = tmem_base + (uint32_t(quarter * 32) << 16) + uint32_t(b * BN);
+            const unsigned char *xslot = xring + (lt % XSLOTS) * BN * 4;
             float tmin = INFINITY;  // threshold pass: minimum over this thread's chunks of the tile
             bool tany = false;
 #pragma unroll 1
@@ -417,10 +461,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 // and vadd = |q|^2, 0, 1: one FMA (integer multiply-add) or negation per element,
                 // then the chunk's minimum. a is monotonic in v (float rounding included), so a
                 // chunk whose minimum fails the threshold has no candidate; the rare chunks with
-                // one test each element. |x|^2 of the CW columns is loaded with the same addresses
-                // in every lane (broadcast loads), before the TMEM load so both latencies overlap;
-                // the |x|^2 arrays hold n_pad >= col0 + CW entries (zero beyond the data rows).
-                // Staging them in shared memory per warp measured no faster (504 against 490 us).
+                // one test each element. |x|^2 of the CW columns comes from the tile's ring slot,
+                // which the producer filled with one bulk copy (zero beyond the data rows): the
+                // same addresses in every lane (shared-memory broadcasts) instead of an L2 round
+                // trip per chunk (the whole 1M x 128 call: 6.95 against 7.06 ms).
                 float v[CW];     // BF16 path: v; byte path: the raw S32 accumulator bits
                 int32_t w[CW];   // byte path: v, exact
                 float amin, vadd = 0.f;
@@ -428,10 +472,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 if constexpr (I8) {
                     int32_t xv[CW];
                     if (l2) {
-                        const int4 *x4 = reinterpret_cast<const int4 *>(p.xxi + col0);
+                        const int4 *x4 = reinterpret_cast<const int4 *>(xslot) + c / 4;
 #pragma unroll
                         for (int i = 0; i < CW / 4; i++) {
-                            const int4 t = __ldg(x4 + i);
+                            const int4 t = x4[i];
                             xv[4 * i] = t.x;
                             xv[4 * i + 1] = t.y;
                             xv[4 * i + 2] = t.z;
@@ -459,10 +503,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
                 } else {
                     float xv[CW];
                     if (l2) {
-                        const float4 *x4 = reinterpret_cast<const float4 *>(p.xx + col0);
+                        const float4 *x4 = reinterpret_cast<const float4 *>(xslot) + c / 4;
 #pragma unroll
                         for (int i = 0; i < CW / 4; i++) {
-                            const float4 t = __ldg(x4 + i);
+                            const float4 t = x4[i];
                             xv[4 * i] = t.x;
                             xv[4 * i + 1] = t.y;
                             xv[4 * i + 2] = t.z;
@@ -522,7 +566,10 @@ __global__ void __launch_bounds__(FILTER_THREADS, 1)
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(tempty + b);
+            if (lane == 0) {
+                mbar_arrive(tempty + b);
+                mbar_arrive(xempty + lt % XSLOTS);
+            }
         }
         if (qvalid) p.cand_cnt[seg] = cnt;
     }
@@ -1284,7 +1331,7 @@ int exact_knn_typed(const hnsw_b200_exact_args_t *a, cudaStream_t s, int64_t cap
     CUtensorMap tmA, tmB;
     if (int rc = make_map(&tmA, B + o_qb, q_pad, kp, BM, bytes)) return rc;
     if (int rc = make_map(&tmB, B + o_xb, n_pad, kp, BN, bytes)) return rc;
-    const size_t smem = STAGES * STAGE_BYTES + 1024 + BAR_BYTES;
+    const size_t smem = STAGES * STAGE_BYTES + XSLOTS * BN * 4 + 1024 + BAR_BYTES;
     XT(cudaFuncSetAttribute(knn_filter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     XT(cudaFuncSetAttribute(knn_filter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int wpb = 4;
