@@ -84,6 +84,10 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_ADMIT_MASKS
 #define HB_ADMIT_MASKS 1
 #endif
+// Filtered layer 0: admit a chunk's neighbours together (exactly the one-by-one outcome).
+#ifndef HB_BATCH_ADMIT_FILT
+#define HB_BATCH_ADMIT_FILT 1
+#endif
 #ifdef HB_PROFILE
 __device__ unsigned long long hb_prof[8];
 #define HB_PROF_DECL unsigned long long hb_t = clock64();
@@ -1431,6 +1435,295 @@ __device__ void cand_refill(const SearchParams &P, Cx &C, CandsT<typename Cx::di
 }
 
 // ----------------------------------------------------------------------- filtered layer-0 search
+// Entries of the descending array [0, m) strictly above (d, id), by one lane (binary search).
+template <typename T>
+__device__ __forceinline__ int lane_count_above(const T *Ad, const int32_t *Ai, int m, T d,
+                                                int32_t id) {
+    int a = 0, b = m;
+    while (a < b) {
+        const int mid = (a + b) >> 1;
+        if (pair_lt_raw(d, id, Ad[mid], Ai[mid])) a = mid + 1;
+        else b = mid;
+    }
+    return a;
+}
+
+// Filtered layer 0: one chunk of new neighbours admitted together, with the same results R, the
+// same candidate set (S and the spill) and the same flags as the reference's one-by-one loop
+// (numba_engine.py:185-195).
+//
+// One by one, neighbour j is pushed to the candidates iff |R| < ef or d_j < worst, and also enters
+// R when allowed; R changes only by allowed neighbours. As for the unfiltered chunk (admit_chunk),
+// R before j is the ef smallest of R0 and the earlier allowed neighbours that passed the first
+// test at the chunk's start, so
+//   pushed_j  <=>  #{x in R0 : x.d <= d_j} + #{allowed i < j passing : d_i <= d_j} < ef,
+// every lane at once; the allowed pushed lanes are R's admissions, merged into R as admit_chunk
+// merges (ef smallest (distance, original id) pairs kept). The candidates are a set popped in
+// (distance, id) order, and S holds its smallest entries below the spill's minimum, so the
+// pushes' order does not matter: the pushes at or above the spill minimum go to the spill; the
+// others merge into S, whose largest entries beyond s_cap then go to the spill (their smallest
+// becomes the spill minimum), as one-by-one inserts would leave them.
+template <class Cx>
+__device__ __forceinline__ void admit_chunk_filtered(const SearchParams &P, Cx &C,
+                                                     CandsT<typename Cx::dist_t> &K, int32_t e,
+                                                     typename Cx::dist_t dj, uint32_t um, int ef,
+                                                     int &r, typename Cx::dist_t &W) {
+    using D = typename Cx::dist_t;
+    const int lane = C.lane;
+    const uint32_t below_me = (1u << lane) - 1u;
+    const int r0 = r;
+    const D W0 = W;
+    const uint32_t pm = __ballot_sync(FULL, ((um >> lane) & 1u) && (r0 < ef || dj < W0));
+    if (!pm) return;
+    const bool inp = (pm >> lane) & 1u;
+    const bool al = inp && is_allowed(P.allowed, e);
+    const uint32_t AM = __ballot_sync(FULL, al);
+    const int32_t eo = inp ? orig_id(P, e) : 0x7fffffff;  // orders R and the candidates
+    int lo = 0, n_eq = 0, eq_lt = 0;  // R0 entries below dj, equal to dj, below (dj, eo)
+    if (inp) {
+        int a = 0, b = r0;
+        while (a < b) {
+            const int m = (a + b) >> 1;
+            if (C.Rd[m] < dj) a = m + 1;
+            else b = m;
+        }
+        lo = a;
+        for (int i = a; i < r0 && C.Rd[i] == dj; i++) {
+            n_eq++;
+            eq_lt += (C.Ri[i] & ID_MASK) < eo;
+        }
+    }
+    uint32_t plem = 0u, ltm = 0u;  // earlier allowed at or below my distance; allowed below me
+    for (uint32_t m = AM; m;) {
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        const D di = __shfl_sync(FULL, dj, i);
+        const int32_t ii = __shfl_sync(FULL, eo, i);
+        const uint32_t bit = 1u << i;
+        plem |= (i < lane && di <= dj) ? bit : 0u;
+        ltm |= (di < dj || (di == dj && ii < eo)) ? bit : 0u;
+    }
+    const bool pushed = inp && lo + n_eq + __popc(plem) < ef;
+    const uint32_t CM = __ballot_sync(FULL, pushed);
+    const uint32_t A = CM & AM;  // R's admissions
+    const bool adm = (A >> lane) & 1u;
+    if (A) {
+        const int pos_r0 = lo + eq_lt;  // R0 entries below (dj, eo)
+        const int fpos = pos_r0 + __popc(ltm & A);
+        const int pmin = __reduce_min_sync(FULL, adm ? pos_r0 : 0x7fffffff);
+        int32_t *rp = C.Rp != C.Ri ? C.Rp : nullptr;
+        // Move R0[p] (p >= pmin) up by the admissions before it, two chunks of 32 a step, highest
+        // first (every read of a step precedes its writes; writes land above the next step's reads).
+        for (int top = r0 - 1; top >= pmin; top -= 64) {
+            const int p1 = top - lane, p2 = top - 32 - lane;
+            const bool a1 = p1 >= pmin, a2 = p2 >= pmin;
+            D d1 = D(0), d2 = D(0);
+            int32_t i1 = 0, i2 = 0, q1 = 0, q2 = 0;
+            if (a1) {
+                d1 = C.Rd[p1];
+                i1 = C.Ri[p1];
+                if (rp) q1 = rp[p1];
+            }
+            if (a2) {
+                d2 = C.Rd[p2];
+                i2 = C.Ri[p2];
+                if (rp) q2 = rp[p2];
+            }
+            int s1 = 0, s2 = 0;
+            for (uint32_t m = A; m;) {
+                const int i = __ffs(m) - 1;
+                m &= m - 1;
+                const int pr = __shfl_sync(FULL, pos_r0, i);
+                s1 += pr <= p1;
+                s2 += pr <= p2;
+            }
+            __syncwarp();
+            if (a1) {
+                C.Rd[p1 + s1] = d1;
+                C.Ri[p1 + s1] = i1;
+                if (rp) rp[p1 + s1] = q1;
+            }
+            if (a2) {
+                C.Rd[p2 + s2] = d2;
+                C.Ri[p2 + s2] = i2;
+                if (rp) rp[p2 + s2] = q2;
+            }
+            __syncwarp();
+        }
+        if (adm) {
+            C.Rd[fpos] = dj;
+            C.Ri[fpos] = eo;
+            if (rp) rp[fpos] = e;
+        }
+        __syncwarp();
+        r = min(ef, r0 + __popc(A));
+        W = C.Rd[r - 1];
+    }
+    // ---- candidates: every pushed lane
+    if (!CM) return;
+    int32_t *sp = C.Sp != C.Si ? C.Sp : nullptr;
+    // at or above the spill minimum: appended to the spill in lane order
+    const bool low = pushed && (K.g == 0 || pair_lt_raw(dj, eo, K.gd, K.gi));
+    const uint32_t LM = __ballot_sync(FULL, low);
+    const uint32_t HM = CM & ~LM;
+    if (HM) {
+        const int idx = K.g + __popc(HM & below_me);
+        if (((HM >> lane) & 1u) && idx < P.spill_cap) {
+            C.spd[idx] = dj;
+            C.spi[idx] = eo;
+            if (C.spp != C.spi) C.spp[idx] = e;
+        }
+        K.g += __popc(HM);
+        if (K.g > P.spill_cap) {
+            C.status |= ST_SPILL;
+            K.g = P.spill_cap;
+        }
+    }
+    if (!LM) return;
+    // below it: merged into S (descending by (distance, original id)); the excess largest of the
+    // merge go to the spill
+    const int s0 = K.s;
+    const int nl = __popc(LM);
+    int s_above = low ? lane_count_above(C.Sd, C.Si, s0, dj, eo) : 0;  // S0 entries above mine
+    int new_above = 0;  // pushed low lanes above mine
+    for (uint32_t m = LM; m;) {
+        const int i = __ffs(m) - 1;
+        m &= m - 1;
+        const D di = __shfl_sync(FULL, dj, i);
+        const int32_t ii = __shfl_sync(FULL, eo, i);
+        new_above += pair_lt_raw(dj, eo, di, ii);
+    }
+    const int rank_new = s_above + new_above;  // my index in the merged descending array
+    const int excess = max(0, s0 + nl - P.s_cap);
+    // S0[p] lies at p + a(p) in the merge, a(p) = pushed entries above it (those with s_above <= p);
+    // p + a(p) grows with p, so the evicted S0 entries (merged index below excess) are a prefix.
+    int x0 = 0;
+    uint32_t E1 = 0u;
+    if (excess > 0) {
+        int a = 0;  // a(lane)
+        for (uint32_t m = LM; m;) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1;
+            a += __shfl_sync(FULL, s_above, i) <= lane;
+        }
+        const bool ev0 = lane < s0 && lane + a < excess;
+        const bool ev1 = low && rank_new < excess;  // pushed entries evicted straight to the spill
+        const uint32_t E0 = __ballot_sync(FULL, ev0);
+        E1 = __ballot_sync(FULL, ev1);
+        x0 = __popc(E0);
+        // A lane may hold both an evicted S0 entry (S0[lane]) and its own evicted pushed entry.
+        D sd0 = D(0);
+        int32_t si0 = 0, sp0 = 0;
+        if (ev0) {
+            sd0 = C.Sd[lane];
+            si0 = C.Si[lane];
+            sp0 = sp ? sp[lane] : si0;
+            const int idx = K.g + lane;
+            if (idx < P.spill_cap) {
+                C.spd[idx] = sd0;
+                C.spi[idx] = si0;
+                if (C.spp != C.spi) C.spp[idx] = sp0;
+            }
+        }
+        if (ev1) {
+            const int idx = K.g + x0 + __popc(E1 & below_me);
+            if (idx < P.spill_cap) {
+                C.spd[idx] = dj;
+                C.spi[idx] = eo;
+                if (C.spp != C.spi) C.spp[idx] = e;
+            }
+        }
+        // the smallest evicted entry (merged index excess - 1) becomes the spill minimum
+        const uint32_t L0 = __ballot_sync(FULL, ev0 && lane + a == excess - 1);
+        const uint32_t L1 = __ballot_sync(FULL, ev1 && rank_new == excess - 1);
+        const int src = __ffs(L0 ? L0 : L1) - 1;
+        const D gd0 = __shfl_sync(FULL, sd0, src), gd1 = __shfl_sync(FULL, dj, src);
+        const int32_t gi0 = __shfl_sync(FULL, si0, src), gi1 = __shfl_sync(FULL, eo, src);
+        K.gd = L0 ? gd0 : gd1;
+        K.gi = L0 ? gi0 : gi1;
+        K.g += excess;
+        if (K.g > P.spill_cap) {
+            C.status |= ST_SPILL;
+            K.g = P.spill_cap;
+        }
+        __syncwarp();
+        // S0[x0 ..) down by x0, lowest chunk first (each chunk read before written; writes land
+        // below the next chunk's reads)
+        if (x0 > 0) {
+            for (int base = x0; base < s0; base += 32) {
+                const int i = base + lane;
+                D d = D(0);
+                int32_t id = 0, ip = 0;
+                if (i < s0) {
+                    d = C.Sd[i];
+                    id = C.Si[i];
+                    if (sp) ip = sp[i];
+                }
+                __syncwarp();
+                if (i < s0) {
+                    C.Sd[i - x0] = d;
+                    C.Si[i - x0] = id;
+                    if (sp) sp[i - x0] = ip;
+                }
+                __syncwarp();
+            }
+        }
+    }
+    // the remaining pushed entries: inserted into S0' = S0[x0 ..) at ins = s_above - x0, the
+    // entries at or after an insertion point moving up by the insertions at or before them
+    const uint32_t RM = LM & ~E1;
+    const int s1 = s0 - x0;
+    if (RM) {
+        const bool mine = (RM >> lane) & 1u;
+        const int ins = s_above - x0;
+        const int pmin = __reduce_min_sync(FULL, mine ? ins : 0x7fffffff);
+        for (int top = s1 - 1; top >= pmin; top -= 64) {
+            const int p1 = top - lane, p2 = top - 32 - lane;
+            const bool a1 = p1 >= pmin, a2 = p2 >= pmin;
+            D d1 = D(0), d2 = D(0);
+            int32_t i1 = 0, i2 = 0, q1 = 0, q2 = 0;
+            if (a1) {
+                d1 = C.Sd[p1];
+                i1 = C.Si[p1];
+                if (sp) q1 = sp[p1];
+            }
+            if (a2) {
+                d2 = C.Sd[p2];
+                i2 = C.Si[p2];
+                if (sp) q2 = sp[p2];
+            }
+            int u1 = 0, u2 = 0;
+            for (uint32_t m = RM; m;) {
+                const int i = __ffs(m) - 1;
+                m &= m - 1;
+                const int pi = __shfl_sync(FULL, ins, i);
+                u1 += pi <= p1;
+                u2 += pi <= p2;
+            }
+            __syncwarp();
+            if (a1) {
+                C.Sd[p1 + u1] = d1;
+                C.Si[p1 + u1] = i1;
+                if (sp) sp[p1 + u1] = q1;
+            }
+            if (a2) {
+                C.Sd[p2 + u2] = d2;
+                C.Si[p2 + u2] = i2;
+                if (sp) sp[p2 + u2] = q2;
+            }
+            __syncwarp();
+        }
+        if (mine) {
+            const int f = rank_new - excess;
+            C.Sd[f] = dj;
+            C.Si[f] = eo;
+            if (sp) sp[f] = e;
+        }
+        __syncwarp();
+    }
+    K.s = s1 + __popc(RM);
+}
+
 // numba_engine._search_layer0_filtered (:151-198): results hold allowed nodes only, the worst of
 // an empty result list is +inf, and the search stops only when the results are full and the
 // closest candidate is strictly farther than the worst.
@@ -1473,10 +1766,14 @@ __device__ void layer0_filtered(const SearchParams &P, Cx &C, int ef, int log2, 
         for (int base = 0; base < cnt; base += 32) {
             const int32_t e = base == 0 ? first_link(nb, P.links0_stride, cnt, lane)
                                         : (base + lane < cnt ? __ldg(nb + base + lane) : -1);
-            const int32_t eo = e >= 0 ? orig_id(P, e) : -1;
             D dj;
             const uint32_t um = mark_and_score<MODE, U8, CFG>(P, C, e, log2, vis_count, dj);
             C.ndist += __popc(um);
+            if (HB_BATCH_ADMIT_FILT) {
+                admit_chunk_filtered(P, C, K, e, dj, um, ef, r, W);
+                continue;
+            }
+            const int32_t eo = e >= 0 ? orig_id(P, e) : -1;
             uint32_t am = __ballot_sync(FULL, ((um >> lane) & 1u) && (r < ef || dj < W));
             while (am) {
                 const int j = __ffs(am) - 1;
