@@ -138,6 +138,9 @@ struct SearchParams {
     const float *vectors;
     const uint8_t *codes;
     const uint8_t *rows8;  // byte mode: the uint8 rows searched
+    // fused rerank: the vectors' uint8 copy (integer vectors in [0, 255]; L2 or inner product,
+    // dim a multiple of 16 up to 128), or NULL
+    const uint8_t *rerank_rows8;
     const int32_t *links0;
     const int32_t *count0;
     const int64_t *upper_offset;
@@ -1809,8 +1812,9 @@ __device__ void layer0_filtered(const SearchParams &P, Cx &C, int ef, int log2, 
 // numba_engine._rerank_batch (:506-530): exact float64 distances from the float32 query to the
 // first m beam entries, best k by (distance, id).
 // internal: R holds internal ids only (unfiltered); otherwise Ri holds the original ids.
+// bytes: the query and the vectors are bytes (P.rerank_rows8, query bytes in C.q4): integer sums.
 template <class Cx>
-__device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m, bool internal) {
+__device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m, bool internal, bool bytes) {
     const int lane = C.lane;
     const int k = P.k;
     int a = 0;
@@ -1819,7 +1823,20 @@ __device__ int rerank_epilogue(const SearchParams &P, Cx &C, int m, bool interna
         const bool has = i < m;
         const int32_t ri = has ? (C.Ri[i] & ID_MASK) : -1;
         const int32_t id = has && internal ? orig_id(P, ri) : ri;  // original id
-        const double d = has ? dist_seq_f64<false>(P, C.Rp[i] & ID_MASK, C.qd) : INFINITY;
+        double d = INFINITY;
+        if (bytes) {
+            if (has) {
+                const uint4 *row = reinterpret_cast<const uint4 *>(
+                    P.rerank_rows8 + int64_t(C.Rp[i] & ID_MASK) * P.dim);
+                const int v4 = P.dim >> 4;
+                uint4 x[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) x[t] = t < v4 ? __ldg(row + t) : make_uint4(0u, 0u, 0u, 0u);
+                d = row_dot_bytes<double>(P, C, x, v4);
+            }
+        } else if (has) {
+            d = dist_seq_f64<false>(P, C.Rp[i] & ID_MASK, C.qd);
+        }
         uint32_t am = __ballot_sync(FULL, has);
         while (am) {
             const int j = __ffs(am) - 1;
@@ -1995,10 +2012,20 @@ __global__ void __launch_bounds__(WPB * 32, min_blocks<MODE, FILT, CFG>())
         int64_t *oi = P.out_ids + int64_t(q) * k;
         double *od = P.out_dists + int64_t(q) * k;
         if (rerank) {
+            // A query whose values are all bytes, over byte vectors, is re-scored in integers
+            // (its bytes replace the searched query's in C.q4): the float64 sums of the reference
+            // are exact on such data, so the distances are the same numbers.
             const float *rq = P.rerank_queries + int64_t(q) * dim;
-            for (int i = lane; i < dim; i += 32) C.qd[i] = double(rq[i]);
+            uint32_t not_byte = P.rerank_rows8 ? 0u : 1u;
+            for (int i = lane; i < dim; i += 32) {
+                const float v = rq[i];
+                C.qd[i] = double(v);
+                if (rintf(v) != v || !(v >= 0.f) || !(v <= 255.f)) not_byte = 1u;
+                else if (P.rerank_rows8) qb[i] = uint8_t(v);
+            }
+            not_byte = __reduce_or_sync(FULL, not_byte);
             __syncwarp();
-            const int a = rerank_epilogue(P, C, min(r, P.k_search), !FILT);
+            const int a = rerank_epilogue(P, C, min(r, P.k_search), !FILT, not_byte == 0u);
             for (int i = lane; i < k; i += 32) {
                 oi[i] = i < a ? int64_t(C.Ai[i]) : -1;
                 od[i] = i < a ? C.Ad[i] : INFINITY;
@@ -2368,6 +2395,10 @@ int search_impl(Handle &h, const hnsw_b200_search_args_t *a, cudaStream_t s, boo
     P.ef_cap = ef_cap;
     P.allowed = a->allowed;
     P.rerank_queries = a->rerank_queries;
+    P.rerank_rows8 = (a->rerank_queries && g.vector_bytes && g.metric != HNSW_B200_COSINE &&
+                      (g.dim & 15) == 0 && g.dim <= 128)
+                         ? g.vector_bytes
+                         : nullptr;
     P.out_ids = a->out_ids;
     P.out_dists = a->out_dists;
     P.out_ctr = a->out_counters;
@@ -2666,6 +2697,10 @@ extern "C" int hnsw_b200_search_noalloc(const hnsw_b200_graph_t *graph,
     P.ef = a->ef;
     P.ef_cap = ef_cap;
     P.rerank_queries = a->rerank_queries;
+    P.rerank_rows8 = (a->rerank_queries && g.vector_bytes && g.metric != HNSW_B200_COSINE &&
+                      (g.dim & 15) == 0 && g.dim <= 128)
+                         ? g.vector_bytes
+                         : nullptr;
     P.out_ids = a->out_ids;
     P.out_dists = a->out_dists;
     P.out_ctr = a->out_counters;
