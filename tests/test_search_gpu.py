@@ -109,6 +109,30 @@ def test_quantized_search_and_fused_rerank_match_reference(name: str, locality: 
         np.testing.assert_array_equal(dists, case[f"dists_r{r}"])
 
 
+@pytest.mark.parametrize("locality", [False, True], ids=["reference_order", "cell_order"])
+def test_fused_rerank_of_byte_and_non_byte_queries_matches_oracle(locality: bool) -> None:
+    """Fused rerank on a graph holding a byte copy of its vectors: query rows whose values are all
+    bytes are re-scored in integers, the others (every second row shifted by 0.25) in float64.
+    Both equal the reference's two steps (the code search's candidates, then the float64 re-score,
+    numba_engine.py:506-530) run by the oracle."""
+    from hnsw_engine_b200 import QuantizedIndex
+    from oracle import cpu
+
+    case = load_golden("search_mix10k")
+    arrays, ep, ml = case_arrays(case, "mix10k")
+    q = np.ascontiguousarray(case["queries"][:64], dtype=np.float32)
+    q[1::2] += 0.25
+    qi = QuantizedIndex(_index(arrays, ep, ml, "l2", 16, locality))
+    ids, dists = qi.batch_search(q, k=10, ef=64, rerank=64)
+    codes = qi.quantizer.encode(np.asarray(arrays["vectors"], dtype=np.float32))
+    code_q = qi.quantizer.transform_queries(q, "l2")
+    cand, _, _ = cpu.search_batch(arrays, ep, ml, code_q, 64, 64, "l2", codes=codes, threads=8)
+    o_ids, o_d = cpu.rerank_batch(np.asarray(arrays["vectors"], dtype=np.float32), q, cand, 10, "l2",
+                                  threads=8)
+    np.testing.assert_array_equal(ids, o_ids)
+    np.testing.assert_array_equal(dists, o_d)
+
+
 @pytest.mark.parametrize("name", ["int_l2", "cont_l2", "cont_ip", "cont_cosine", "mix10k_filtered"])
 def test_single_query_search_matches_reference_fixtures(name: str) -> None:
     """HNSWIndex.search, one query at a time (the latency path when unfiltered), against the
