@@ -84,10 +84,6 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_GROUP_ROWS
 #define HB_GROUP_ROWS 1
 #endif
-// Layer-0 bitmap marks: one atomic per distinct bitmap word of a chunk instead of one per lane.
-#ifndef HB_WORD_ATOMICS
-#define HB_WORD_ATOMICS 0
-#endif
 // Batched admission: one pass over the chunk's candidates builds each lane's "below me" masks
 // (3.5% faster than counting over the admitted set in a second pass: 3.45 -> 3.33 ms at ef = 192 on
 // the 1M mixture, identical results).
@@ -701,19 +697,6 @@ __device__ __forceinline__ uint32_t mark_chunk(const SearchParams &P, Cx &C, int
     const bool has = e >= 0;
     const uint32_t hmask = __ballot_sync(FULL, has);
     int ins = 0;
-#if HB_WORD_ATOMICS
-    if (has && log2 == 0) {  // one atomic per bitmap word, carrying the bits of every lane on it
-        const uint32_t same = __match_any_sync(hmask, e);
-        const uint32_t wm = __match_any_sync(hmask, e >> 5);
-        const uint32_t bit = 1u << (e & 31);
-        const uint32_t bits = __reduce_or_sync(wm, bit);
-        const int lead = __ffs(wm) - 1;
-        uint32_t old = 0u;
-        if (C.lane == lead) old = atomicOr(C.vbits + (e >> 5), bits);
-        old = __shfl_sync(wm, old, lead);
-        ins = (__ffs(same) - 1 == C.lane && !(old & bit)) ? 1 : 0;
-    } else
-#endif
     if (has) {
         uint32_t same = __match_any_sync(hmask, e);
         if (__ffs(same) - 1 == C.lane) {
@@ -837,14 +820,16 @@ __device__ __forceinline__ uint32_t mark_score_lane_rows(const SearchParams &P, 
     return um;
 }
 
-// Byte rows of at most 128 bytes (dim a multiple of 16), gathered a row per group of eight lanes:
-// in load t, lane l fetches 16-byte piece l & 7 of the row held by lane 4t + (l >> 3), so each
-// load instruction touches four rows instead of 32 and the L1 serves a chunk's rows in an eighth
-// of the wavefronts. The loads are issued before the visited marks resolve, as in
-// mark_score_lane_rows. Each lane sums its eight pieces against the matching piece of the query
-// (pieces beyond the row are zero on both sides); three exchange rounds over the group leave lane
-// (g, p) with the whole sum of row 4p + g, and one shuffle hands it to the lane holding that
-// neighbour. Integer sums, so the values equal row_dot_bytes' bit for bit.
+// Byte rows of exactly 128 bytes, gathered a row per group of eight lanes: in load t, lane l
+// fetches 16-byte piece l & 7 of the row held by lane 4t + (l >> 3), so each load instruction
+// touches four 128-byte lines instead of 32 and the L1 serves a chunk's rows in an eighth of the
+// wavefronts. The loads are issued before the visited marks resolve, as in mark_score_lane_rows.
+// Each lane sums its eight pieces against the matching piece of the query; three exchange rounds
+// over the group leave lane (g, p) with the whole sum of row 4p + g, and one shuffle hands it to
+// the lane holding that neighbour. Integer sums, so the values equal row_dot_bytes' bit for bit.
+// (A form for any row of at most 128 bytes, with the pieces beyond the row predicated off and the
+// row offset multiplied by dim, measured slower than the row-per-lane gather on the 1M mixture:
+// 3.35 against 3.28 ms at ef = 192; this one takes 2.95 ms.)
 template <class Cx>
 __device__ __forceinline__ uint32_t mark_score_group_rows(const SearchParams &P, Cx &C, int32_t e,
                                                           int log2, int &vis_count,
@@ -852,17 +837,15 @@ __device__ __forceinline__ uint32_t mark_score_group_rows(const SearchParams &P,
     using D = typename Cx::dist_t;
     const int lane = C.lane;
     const int g = lane >> 3, p = lane & 7;
-    const int v4 = P.dim >> 4;
     uint4 x[8];
 #pragma unroll
     for (int t = 0; t < 8; t++) {
         // a lane with no neighbour lends row 0: its sum lands in a slot nobody reads
         const uint32_t et = uint32_t(max(__shfl_sync(FULL, e, 4 * t + g), 0));
-        x[t] = p < v4 ? __ldg(reinterpret_cast<const uint4 *>(P.rows8 + uint64_t(et) * P.dim) + p)
-                      : make_uint4(0u, 0u, 0u, 0u);
+        x[t] = __ldg(reinterpret_cast<const uint4 *>(P.rows8 + (uint64_t(et) << 7)) + p);
     }
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
-    const uint4 q = p < v4 ? reinterpret_cast<const uint4 *>(C.q4)[p] : make_uint4(0u, 0u, 0u, 0u);
+    const uint4 q = reinterpret_cast<const uint4 *>(C.q4)[p];
     uint32_t s[8];
     if (P.metric == HNSW_B200_L2) {
 #pragma unroll
@@ -943,7 +926,7 @@ __device__ __forceinline__ uint32_t mark_and_score(const SearchParams &P, Cx &C,
     if (MODE == MODE_BYTES && HB_LANE_ROWS && C.lane_rows) {
         // stage_bytes() gives every lane-row search of a byte kernel its staging slot
         if constexpr (cfg_stage(CFG)) return mark_score_lane_rows_staged(P, C, e, log2, vis_count, dj);
-        if constexpr (HB_GROUP_ROWS) return mark_score_group_rows(P, C, e, log2, vis_count, dj);
+        if (HB_GROUP_ROWS && P.dim == 128) return mark_score_group_rows(P, C, e, log2, vis_count, dj);
         return mark_score_lane_rows(P, C, e, log2, vis_count, dj);
     }
     const uint32_t um = mark_chunk(P, C, e, log2, vis_count);
