@@ -8,10 +8,10 @@
 // rounding is of no consequence; ties go to the lower pivot index. A block of 128 threads takes
 // 16 queries; each thread holds two pivots of the current group of 256 and accumulates their dot
 // products with all 16 queries. Queries and pivots arrive 32 dimensions at a time through shared
-// memory: rows read whole (coalesced) and stored transposed, the queries read back as float4
-// broadcasts, the pivots one word per thread (the pivot tile's rows are padded by one word, so
-// the transposing stores and the reads are free of bank conflicts). 10,000 queries make 625
-// blocks: one wave.
+// memory: rows read whole (coalesced; the pivots as 16-byte pieces when the rows allow) and stored
+// transposed, the queries read back as float4 broadcasts, the pivots one word per thread (the
+// pivot tile's rows are padded by one word, so the transposing stores and the reads are free of
+// bank conflicts). 10,000 queries make 625 blocks: one wave.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,7 +35,7 @@ constexpr int DC = 32;        // dimensions per staged chunk
 __global__ void __launch_bounds__(THREADS) start_priority_kernel(
     const float *__restrict__ queries, int32_t nq, int32_t dim, const float *__restrict__ pivots,
     int32_t n_cells, const double *__restrict__ cost, const int32_t *__restrict__ ef, float scale,
-    int32_t *__restrict__ cells, int32_t *__restrict__ priority) {
+    int32_t *__restrict__ cells, int32_t *__restrict__ priority, bool vec4) {
     __shared__ __align__(16) float qs[DC][QT];  // [dimension][query]
     __shared__ float ps[DC][GROUP + 1];         // [dimension][pivot of the group]
     __shared__ float wd[THREADS / 32][QT];
@@ -65,10 +65,30 @@ __global__ void __launch_bounds__(THREADS) start_priority_kernel(
                 const int qi = q0 + i, dd = d0 + d;
                 qs[d][i] = (qi < nq && dd < dim) ? queries[int64_t(qi) * dim + dd] : 0.f;
             }
-            for (int e = t; e < GROUP * DC; e += THREADS) {  // and 256 pivots x 32 dimensions
-                const int j = e / DC, d = e % DC;
-                const int pj = g0 + j, dd = d0 + d;
-                ps[d][j] = (pj < n_cells && dd < dim) ? __ldg(pivots + int64_t(pj) * dim + dd) : 0.f;
+            if (vec4 && d0 + DC <= dim) {
+                // and 256 pivots x 32 dimensions, as 16-byte pieces: sixteen loads a thread in two
+                // batches of eight (80 registers, so the 625 blocks of 10,000 queries stay one
+                // wave), eight threads to a pivot's 128 bytes; piece k of pivot j lands in rows
+                // 4k..4k+3 of the tile, banks 4k + c + j (mod 32), distinct across a warp
+#pragma unroll 8
+                for (int e = t; e < GROUP * DC / 4; e += THREADS) {
+                    const int j = e / (DC / 4), k = e % (DC / 4);
+                    const int pj = g0 + j;
+                    const float4 v = pj < n_cells
+                                         ? __ldg(reinterpret_cast<const float4 *>(
+                                                     pivots + int64_t(pj) * dim + d0) + k)
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+                    ps[4 * k][j] = v.x;
+                    ps[4 * k + 1][j] = v.y;
+                    ps[4 * k + 2][j] = v.z;
+                    ps[4 * k + 3][j] = v.w;
+                }
+            } else {
+                for (int e = t; e < GROUP * DC; e += THREADS) {  // one word at a time
+                    const int j = e / DC, d = e % DC;
+                    const int pj = g0 + j, dd = d0 + d;
+                    ps[d][j] = (pj < n_cells && dd < dim) ? __ldg(pivots + int64_t(pj) * dim + dd) : 0.f;
+                }
             }
             __syncthreads();
             const int nd = min(DC, dim - d0);
@@ -160,7 +180,8 @@ extern "C" int hnsw_b200_start_priority(const float *queries, int64_t nq, int32_
         return hb::fail(HNSW_B200_EINVAL, "start_priority: null pointer");
     const int blocks = int((nq + hbs::QT - 1) / hbs::QT);
     hbs::start_priority_kernel<<<blocks, hbs::THREADS, 0, static_cast<cudaStream_t>(stream)>>>(
-        queries, int32_t(nq), dim, pivots, n_cells, cost, ef, scale, cells, priority);
+        queries, int32_t(nq), dim, pivots, n_cells, cost, ef, scale, cells, priority,
+        (dim & 3) == 0 && (reinterpret_cast<uintptr_t>(pivots) & 15) == 0);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return hb::fail(HNSW_B200_ECUDA, std::string("start_priority: ") + cudaGetErrorString(e));
     return HNSW_B200_OK;

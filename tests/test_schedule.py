@@ -34,6 +34,21 @@ def test_cells_are_the_nearest_pivots() -> None:
     assert (prio == 0).all()  # nothing learned yet
 
 
+def test_byte_valued_cells_are_exact_at_d128() -> None:
+    # the benchmark's shape (256 pivots x 128 dimensions, pivots staged as 16-byte pieces):
+    # byte-valued data make every float32 sum exact, so the cells equal the float64 argmin,
+    # ties to the lower pivot
+    rng = np.random.default_rng(5)
+    piv = rng.integers(0, 256, (256, 128)).astype(np.float32)
+    piv[17] = piv[3]  # a tied pair
+    q = rng.integers(0, 256, (700, 128)).astype(np.float32)
+    q[:5] = piv[3]
+    cells, _ = _start(piv, q, np.full(700, 64))
+    d = ((q[:, None, :].astype(np.float64) - piv[None, :, :]) ** 2).sum(-1)
+    assert cells.tolist() == d.argmin(1).tolist()
+    assert (cells[:5] == 3).all()
+
+
 def test_equal_distances_pick_the_lower_pivot() -> None:
     piv = np.array([[0, 0], [1, 0], [0, 0], [1, 0]], np.float32)
     q = np.array([[0, 0], [1, 0], [0.5, 0]], np.float32)
