@@ -84,6 +84,10 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_GROUP_ROWS
 #define HB_GROUP_ROWS 1
 #endif
+// Batched admission: rank a candidate in R by a binary search whose step count is uniform.
+#ifndef HB_UNIFORM_RANK
+#define HB_UNIFORM_RANK 0
+#endif
 // Float64 rows: prefetch a row's lines into L1 before its sequential sum (prefetch_row_l1).
 // Identical results; t1m (1M x 100 cosine, 10K queries) ef = 256 10.81 -> 9.59 ms, its int8 codes
 // with the float64 rerank at ef = 128 6.72 -> 6.47 ms, the 1M mixture in float64 at ef = 192
@@ -1116,12 +1120,24 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
     const bool inc = (cm >> lane) & 1u;
     int lo = 0, n_eq = 0, eq_lt = 0;
     if (inc) {
+#if HB_UNIFORM_RANK
+        // lo: entries of R0 with distance below dj, in a number of steps that depends on r0 alone
+        // (the same for every lane): the answer stays within [a, a + n]
+        int a = 0;
+        for (int n = r0; n > 1;) {
+            const int half = n >> 1;
+            a = C.Rd[a + half - 1] < dj ? a + half : a;
+            n -= half;
+        }
+        if (r0 > 0 && C.Rd[a] < dj) a++;
+#else
         int a = 0, b = r0;  // lo: entries of R0 with distance below dj
         while (a < b) {
             const int m = (a + b) >> 1;
             if (C.Rd[m] < dj) a = m + 1;
             else b = m;
         }
+#endif
         lo = a;
         if (a < r0 && C.Rd[a] == dj) {  // equal distances (rare): rank by original id
             const int32_t eo = orig_id(P, e);
