@@ -432,6 +432,20 @@ __device__ __forceinline__ void shift_down(T *Ad, int32_t *Ai, int pos, int m, i
 }
 
 // ---------------------------------------------------------------------------------------- visited
+// Length of the prefix of [0, m) on which pred holds (pred true on a prefix, false after), by a
+// binary search whose step count depends on m alone: the lanes of a warp never diverge in it.
+template <class F>
+__device__ __forceinline__ int uniform_prefix(int m, F pred) {
+    int a = 0;  // the answer stays within [a, a + n]
+    for (int n = m; n > 1;) {
+        const int half = n >> 1;
+        a = pred(a + half - 1) ? a + half : a;
+        n -= half;
+    }
+    if (m > 0 && pred(a)) a++;
+    return a;
+}
+
 __device__ __forceinline__ void vis_clear(int32_t *tab, int log2, int lane) {
     int4 *t4 = reinterpret_cast<int4 *>(tab);
     const int n4 = (1 << log2) >> 2;
@@ -1123,15 +1137,8 @@ __device__ __forceinline__ void admit_chunk(const SearchParams &P, Cx &C, int32_
     int lo = 0, n_eq = 0, eq_lt = 0;
     if (inc) {
 #if HB_UNIFORM_RANK
-        // lo: entries of R0 with distance below dj, in a number of steps that depends on r0 alone
-        // (the same for every lane): the answer stays within [a, a + n]
-        int a = 0;
-        for (int n = r0; n > 1;) {
-            const int half = n >> 1;
-            a = C.Rd[a + half - 1] < dj ? a + half : a;
-            n -= half;
-        }
-        if (r0 > 0 && C.Rd[a] < dj) a++;
+        // lo: entries of R0 with distance below dj (the same step count in every lane)
+        const int a = uniform_prefix(r0, [&](int i) { return C.Rd[i] < dj; });
 #else
         int a = 0, b = r0;  // lo: entries of R0 with distance below dj
         while (a < b) {
@@ -1545,6 +1552,9 @@ __device__ void cand_refill(const SearchParams &P, Cx &C, CandsT<typename Cx::di
 template <typename T>
 __device__ __forceinline__ int lane_count_above(const T *Ad, const int32_t *Ai, int m, T d,
                                                 int32_t id) {
+#if HB_UNIFORM_RANK
+    return uniform_prefix(m, [&](int i) { return pair_lt_raw(d, id, Ad[i], Ai[i]); });
+#else
     int a = 0, b = m;
     while (a < b) {
         const int mid = (a + b) >> 1;
@@ -1552,6 +1562,7 @@ __device__ __forceinline__ int lane_count_above(const T *Ad, const int32_t *Ai, 
         else b = mid;
     }
     return a;
+#endif
 }
 
 // Filtered layer 0: one chunk of new neighbours admitted together, with the same results R, the
@@ -1587,12 +1598,16 @@ __device__ __forceinline__ void admit_chunk_filtered(const SearchParams &P, Cx &
     const int32_t eo = inp ? orig_id(P, e) : 0x7fffffff;  // orders R and the candidates
     int lo = 0, n_eq = 0, eq_lt = 0;  // R0 entries below dj, equal to dj, below (dj, eo)
     if (inp) {
+#if HB_UNIFORM_RANK
+        const int a = uniform_prefix(r0, [&](int i) { return C.Rd[i] < dj; });
+#else
         int a = 0, b = r0;
         while (a < b) {
             const int m = (a + b) >> 1;
             if (C.Rd[m] < dj) a = m + 1;
             else b = m;
         }
+#endif
         lo = a;
         for (int i = a; i < r0 && C.Rd[i] == dj; i++) {
             n_eq++;
