@@ -84,6 +84,13 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_GROUP_ROWS
 #define HB_GROUP_ROWS 1
 #endif
+// Filtered searches gather rows before the visited marks only above this allowed share. With the
+// group gather, gathering at every share measured mixed on the 1M mixture (10K queries, one call):
+// Bernoulli p = 0.03 ef = 64 49.4 -> 43.8 ms and p = 0.01 ef = 192 657 -> 636 ms, but p = 0.03
+// ef = 192 160 -> 167 ms and p = 0.01 ef = 64 165 -> 172 ms; the 5% cut stays.
+#ifndef HB_LANE_ROWS_MIN_P
+#define HB_LANE_ROWS_MIN_P 0.05
+#endif
 // Batched admission (unfiltered and filtered): rank a candidate in R (and in the filtered
 // candidates S) by a binary search whose step count depends on the array's length alone, so the
 // lanes never diverge in it (uniform_prefix). Identical results; 1M mixture, 10K queries: ef = 192
@@ -2447,7 +2454,7 @@ int search_impl(Handle &h, const hnsw_b200_search_args_t *a, cudaStream_t s, boo
     // One lane per neighbour's row: a win unless the filter is very selective, where most rows it
     // would fetch early belong to neighbours already visited.
     const double p = filt ? std::max(double(a->allowed_fraction), 1.0 / double(g.n)) : 1.0;
-    const int lane_rows = (!filt || p >= 0.05) ? 1 : 0;
+    const int lane_rows = (!filt || p >= HB_LANE_ROWS_MIN_P) ? 1 : 0;
     const size_t wb = warp_smem_bytes(ef_cap, g.dim, filt, s_cap, krr, g.node_ids != nullptr,
                                       stage_bytes(mode, cfg, lane_rows, g.dim));
     const bool use_mlp = a->stop_mlp != nullptr && !filt;
