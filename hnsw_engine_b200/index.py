@@ -116,8 +116,8 @@ class HNSWIndex:
     Open one with :meth:`load_native` (a ``save_native`` directory) or :meth:`from_arrays`.
     Constructor parameters mirror the reference's (``index.py:115-149``); only ``ef_search`` and
     ``metric`` affect searching. Extensions: ``device``, and ``locality`` (store the graph on the
-    GPU in a cell order for memory locality; ``None`` turns it on from 65,536 nodes when the vectors
-    are integers in [0, 255]; results are the same either way).
+    GPU in a cell order for memory locality; ``None`` turns it on from 65,536 nodes; results are
+    the same either way).
     """
 
     def __init__(

@@ -1,13 +1,14 @@
 """Small, fixed cases of the two hot kernels for profilers (the commands in ``profiles/``).
 
-    python -m hnsw_engine_b200.profile_cases search --nq 2000 --ef 192 [--stop]
+    python -m hnsw_engine_b200.profile_cases search --nq 2000 --ef 192 [--stop] [--workload t1m]
     python -m hnsw_engine_b200.profile_cases exact --nq 1024 [--image] [--calls 2]
 
-``search``: the 1M x 128 mixture graph with ``nq`` of its benchmark queries, three synchronous
-searches at ``ef`` (the learned stop with the shipped network when ``--stop``), autotuning off, so
-the search kernel's launches are the 3 searches in order (with the start order's launches before
-each when ``nq >= 4096``). ``exact``: the tensor-core exact k-NN (k = 100) of ``nq`` mixture
-queries over the 1M x 128 mixture rows (``--image``: 60K x 784 image-like rows), ``calls`` times;
+``search``: the 1M x 128 mixture graph (``--workload t1m``: the 1M x 100 Student-t cosine graph,
+float64 rows) with ``nq`` of its benchmark queries, three synchronous searches at ``ef`` (the
+learned stop with the shipped network when ``--stop``), autotuning off, so the search kernel's
+launches are the 3 searches in order (with the start order's launches before each when
+``nq >= 4096``). ``exact``: the tensor-core exact k-NN (k = 100) of ``nq`` mixture queries over the
+1M x 128 mixture rows (``--image``: 60K x 784 image-like rows), ``calls`` times;
 each call launches the filter kernel twice (the prefix pass, then every row).
 """
 
@@ -24,18 +25,18 @@ from .index import HNSWIndex
 from .validation import prepare
 
 
-def search_case(nq: int, ef: int, stop: bool) -> None:
+def search_case(nq: int, ef: int, stop: bool, workload: str = "mix1m") -> None:
     from .train_stop import load_or_train
 
-    meta, arrays = graphs.open_workload("mix1m")
+    meta, arrays = graphs.open_workload(workload)
     params = {k: v for k, v in meta["params"].items() if k != "engine"}
     g = HNSWIndex.from_arrays(arrays, int(meta["entry_point"]), int(meta["max_level"]),
                               **params).device_graph
     g.autotune = False
-    q = torch.from_numpy(prepare(graphs.workload_queries("mix1m", nq=nq), "l2")).cuda()
+    q = torch.from_numpy(prepare(graphs.workload_queries(workload, nq=nq), meta["params"]["metric"])).cuda()
     kw = {}
     if stop:
-        net = load_or_train("mix1m")
+        net = load_or_train(workload)
         kw["stop"] = (net.packed(), net.threshold, net.slope, net.slope_from)
     for _ in range(3):
         ids, d, c = g.search(q, 10, ef, **kw)
@@ -67,9 +68,10 @@ def main() -> None:
     p.add_argument("--stop", action="store_true")
     p.add_argument("--image", action="store_true")
     p.add_argument("--calls", type=int, default=1)
+    p.add_argument("--workload", default="mix1m", help="search: the graph (mix1m, or t1m for float64 rows)")
     a = p.parse_args()
     if a.case == "search":
-        search_case(a.nq, a.ef, a.stop)
+        search_case(a.nq, a.ef, a.stop, a.workload)
     else:
         exact_case(a.nq, a.image, a.calls)
 

@@ -337,8 +337,9 @@ def test_overflow_retries_keep_results_in_start_order() -> None:
 
 
 def test_start_order_without_cell_order_changes_no_result() -> None:
-    """A large float graph (no cell order: the float64 kernel) gets pivots for the start order
-    alone; fixed and per-query ef give row order's ids, distances and counters."""
+    """A large float graph kept in the reference node order (locality=False; by default it gets the
+    cell order like any large graph) gets pivots for the start order alone; fixed and per-query ef
+    give row order's ids, distances and counters."""
     import torch
 
     from hnsw_engine_b200 import graphs, synthetic
@@ -346,7 +347,8 @@ def test_start_order_without_cell_order_changes_no_result() -> None:
     from hnsw_engine_b200.validation import prepare
 
     arrays, ep, ml, metric = _workload("t100k")
-    g = _index(arrays, ep, ml, metric, 16).device_graph
+    assert _index(arrays, ep, ml, metric, 16).device_graph.locality
+    g = _index(arrays, ep, ml, metric, 16, locality=False).device_graph
     assert g._schedule is not None and not g.locality
     q = torch.from_numpy(prepare(graphs.workload_queries("t100k", nq=MIN_QUERIES), metric)).cuda()
     pq = torch.from_numpy(synthetic.per_query_ef(MIN_QUERIES, seed=3, low=16, high=128)).cuda()
