@@ -91,6 +91,11 @@ constexpr int WPB = 4;  // warps per block
 #ifndef HB_LANE_ROWS_MIN_P
 #define HB_LANE_ROWS_MIN_P 0.05
 #endif
+// Byte codes in float64 sums: read four codes a load (dim a multiple of 4). Identical results;
+// int8 codes of the 1M x 100 cosine graph with the float64 rerank at ef = 128: 6.31 -> 6.16 ms.
+#ifndef HB_CODE_WORDS
+#define HB_CODE_WORDS 1
+#endif
 // Batched admission (unfiltered and filtered): rank a candidate in R (and in the filtered
 // candidates S) by a binary search whose step count depends on the array's length alone, so the
 // lanes never diverge in it (uniform_prefix). Identical results; 1M mixture, 10K queries: ef = 192
@@ -536,6 +541,27 @@ __device__ __forceinline__ double dist_seq_f64(const SearchParams &P, int64_t e,
         }
     } else {
         const uint8_t *x = P.codes + e * dim;
+#if HB_CODE_WORDS
+        if ((dim & 3) == 0) {  // four codes a load (rows start on 4-byte boundaries), same order
+            const uint32_t *x4 = reinterpret_cast<const uint32_t *>(x);
+            const bool l2 = P.metric == HNSW_B200_L2;
+            for (int i = 0; i < dim; i += 4) {
+                const uint32_t w = __ldg(x4 + (i >> 2));
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const double c = double((w >> (8 * u)) & 0xffu);
+                    if (l2) {
+                        const double t = __dsub_rn(c, q[i + u]);
+                        acc = __dadd_rn(acc, __dmul_rn(t, t));
+                    } else {
+                        acc = __dadd_rn(acc, __dmul_rn(c, q[i + u]));
+                    }
+                }
+            }
+            if (l2) return acc;
+            return P.metric == HNSW_B200_IP ? -acc : __dsub_rn(1.0, acc);
+        }
+#endif
         if (P.metric == HNSW_B200_L2) {
             for (int i = 0; i < dim; i++) {
                 double t = __dsub_rn((double)__ldg(x + i), q[i]);
